@@ -1,0 +1,422 @@
+"""Benchmark: exact triangle counting (Bit-BSR build + hybrid count) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+                    [--workload stencil27_64|er_16384|rmat22_deg] [--tile 0|32|128]
+
+A step is one pass of the hot path over one graph: build the Bit-BSR from the raw
+undirected edge list (orient, dedup, tile) and count its triangles.  The default
+workload is the 27-point stencil on a 64^3 grid (262,144 vertices, 3,298,428 edges,
+natural lexicographic order, 16x128 tiles; 11,049,696 triangles).  The metric is
+unique undirected edges per second (whole job; N ranks each count a replica of the
+graph: weak scaling, no data-path collective).
+
+  value      device-resident edge list in HBM, L2 flushed (512 MB write) before
+             every timed step, CUDA events around each step, max over ranks
+  e2e        the same through the public API with host buffers: H2D of the pinned
+             edge list, build, count, D2H of the count, every step
+  roofline   the count kernel (dominant kernel of the step at this size) against
+             the measured HBM copy bandwidth
+  cpu_baseline   the reference's own cpu_tc_intersection_lower_triangular
+             (oracle/_ref/libref_cpu.so, all host threads) on the same L
+  --impl reference   times that same reference CPU path as the reference arm
+
+Only rank 0 prints, and only one JSON line, to stdout.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "btc-tc-artifact_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "exact_tc_edges_per_s"
+UNIT = "edges/s"
+L2_FLUSH_BYTES = 512 << 20
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback 6.65 TB/s"
+
+
+def workload(name: str):
+    from btc_b200 import graphs as G
+    if name == "stencil27_64":
+        src, dst, n = G.stencil27(64)
+        return src, dst, n, dict(workload="27-point stencil 64^3, natural order", tile_cols=128,
+                                 expected=11049696)
+    if name == "er_16384":
+        src, dst, n = G.erdos_renyi(16384, 16, seed=1)
+        return src, dst, n, dict(workload="Erdos-Renyi n=16384 mean degree 16 seed 1",
+                                 tile_cols=0, expected=None)
+    if name == "rmat22_deg":
+        src, dst, n = G.rmat(22, 16, seed=7)
+        return src, dst, n, dict(workload="R-MAT scale 22 ef 16 seed 7, GPU descending-degree order",
+                                 tile_cols=128, expected=None, orient_degree=True)
+    raise SystemExit(f"unknown workload {name}")
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle samples during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+               "-lms", "50"]
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.device_index).uuid)
+            cmd += ["-i", uuid if uuid.startswith("GPU-") else f"GPU-{uuid}"]
+        except Exception:
+            cmd += ["-i", str(self.device_index)]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                         text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception as e:  # no nvidia-smi
+            log("clock sampler unavailable:", e)
+            self.proc = None
+        time.sleep(0.15)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.1)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            parts = [p.strip() for p in l.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def launches_per_step(n: int, tile_cols: int, orient_degree: bool, m: int) -> int:
+    """Kernels the engine launches per build + count (see csrc/capi.cu build_into)."""
+    R = (n + 15) // 16
+    ncb = (n + tile_cols - 1) // tile_cols
+    t_bits = max(R - 1, 0).bit_length() + max(ncb - 1, 0).bit_length()
+    passes = -(-t_bits // 8)
+    k = 1 + 3 * passes + 2 + 1 + 1  # keys, sort, segment (2), fill, indptr
+    if orient_degree:
+        db = max(1, (2 * m).bit_length())
+        k += 1 + 1 + 1 + 3 * (-(-db // 8)) + 1  # degree, rank keys, set count, sort, scatter
+    return k + 1  # count
+
+
+def cpu_reference(rowptr, col, m_lower, budget_s=10.0):
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    O.ref_cpu_count(rowptr, col, threads)  # warm-up
+    times = []
+    t_end = time.perf_counter() + budget_s
+    while True:
+        t0 = time.perf_counter()
+        cnt = O.ref_cpu_count(rowptr, col, threads)
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() > t_end or len(times) >= 50:
+            break
+    t = statistics.median(times)
+    return cnt, t, threads, len(times)
+
+
+def run_reference(args, rank, world):
+    """Reference arm: the reference's CPU path on the host cores (rank 0 only)."""
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    src, dst, n, meta = workload(args.workload)
+    if not O.ref_cpu_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_cpu.so not built"}))
+        return
+    rp, col, _ = O.lower_csr(src, dst, n)
+    m_lower = len(col)
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        O.ref_cpu_count(rp, col, threads)
+    times = []
+    cnt = None
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        cnt = O.ref_cpu_count(rp, col, threads)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = m_lower * args.steps / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic", "config": {"workload": meta["workload"], "edges": m_lower,
+                                        "count": cnt, "parallelism": f"openmp{threads}"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"full graph, {args.steps} counts of the lower CSR"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--workload", default="stencil27_64")
+    ap.add_argument("--tile", type=int, default=None)
+    ap.add_argument("--no-ref-gpu", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=8.0)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from btc_b200 import BitBSR
+    src, dst, n, meta = workload(args.workload)
+    tile = args.tile if args.tile is not None else meta["tile_cols"]
+    odeg = bool(meta.get("orient_degree", False))
+    m_in = len(src)
+    h_src = torch.from_numpy(src).pin_memory()
+    h_dst = torch.from_numpy(dst).pin_memory()
+    d_src = h_src.cuda()
+    d_dst = h_dst.cuda()
+    np_src, np_dst = h_src.numpy(), h_dst.numpy()
+    stream = torch.cuda.current_stream()
+
+    g = BitBSR(d_src, d_dst, n, tile, orient_degree=odeg, stream=stream)
+    tile = g.tile_cols
+    m_lower = g.num_edges
+    expected = meta["expected"]
+    first = g.count(stream=stream)
+    if expected is not None and first != expected:
+        raise SystemExit(f"count {first} != expected {expected}")
+    expected = first
+    info = g.info()
+    B = int(info.bcsr.num_blocks)
+    R = int(info.bcsr.n_row_blocks)
+    tw_bytes = 2 * tile  # 16 rows x tile bits / 8
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    d_out = torch.zeros(1, dtype=torch.int64, device="cuda")
+
+    def step_device():
+        g.rebuild(d_src, d_dst, n, tile, orient_degree=odeg, stream=stream)
+        g.count_async(stream=stream, d_out=d_out.data_ptr())
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        step_device()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        for e0, e1 in ev:
+            flush.zero_()
+            e0.record(stream)
+            step_device()
+            e1.record(stream)
+        torch.cuda.synchronize()
+    step_ms = [e0.elapsed_time(e1) for e0, e1 in ev]
+    total_ms = sum(step_ms)
+    if int(d_out.item()) != expected:
+        raise SystemExit("count mismatch in timed loop")
+    if dist:
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    torch.cuda.synchronize()
+
+    # ---- phase times (same L2 flush): count kernel alone, build alone ----------
+    reps = min(args.steps, 100)
+    t_count, t_build = [], []
+    for _ in range(reps):
+        flush.zero_()
+        cnt, ms = g.count(stream=stream, timing=True)
+        assert cnt == expected
+        t_count.append(ms)
+        flush.zero_()
+        b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        b0.record(stream)
+        g.rebuild(d_src, d_dst, n, tile, orient_degree=odeg, stream=stream)
+        b1.record(stream)
+        torch.cuda.synchronize()
+        t_build.append(b0.elapsed_time(b1))
+    warm = []
+    for _ in range(20):
+        cnt, ms = g.count(stream=stream, timing=True)
+        warm.append(ms)
+    tc_warm = statistics.median(warm)
+    tc = statistics.median(t_count) / 1e3
+    tb = statistics.median(t_build) / 1e3
+
+    # ---- e2e through the public API with host buffers -----------------------
+    e2e_steps = min(args.steps, 100)
+    for _ in range(3):
+        g.rebuild(np_src, np_dst, n, tile, orient_degree=odeg, stream=stream)
+        assert g.count(stream=stream) == expected
+    torch.cuda.synchronize()
+    e2e_ms = []
+    for _ in range(e2e_steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        g.rebuild(np_src, np_dst, n, tile, orient_degree=odeg, stream=stream)
+        cnt = g.count(stream=stream)
+        e1.record(stream)
+        e1.synchronize()
+        assert cnt == expected
+        e2e_ms.append(e0.elapsed_time(e1))
+    e2e_total = sum(e2e_ms)
+    if dist:
+        t = torch.tensor([e2e_total], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+
+    # ---- roofline of the count kernel ----------------------------------------
+    hbm, peak_src = peaks()
+    bytes_count = 4 * (R + 1) + 8 * B + tw_bytes * B + 8
+    bytes_build = 8 * m_in + 4 * (R + 1) + 8 * B + tw_bytes * B
+    achieved = bytes_count / tc / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", f"count_{tile}_{args.workload}.json")
+    if os.path.exists(prof):
+        with open(prof) as f:
+            traffic = json.load(f).get("dram_bytes_per_launch")
+
+    line = {
+        "metric": METRIC,
+        "value": world * m_lower * args.steps / (total_ms / 1e3),
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "int32",
+        "data": "synthetic",
+        "config": {"workload": meta["workload"], "vertices": n, "edges": m_lower,
+                   "input_pairs": m_in, "tile": f"16x{tile}", "tiles": B, "triangles": expected,
+                   "orientation": "descending degree" if odeg else "natural id",
+                   "parallelism": f"replica x{world}" if world > 1 else "single GPU",
+                   "l2": "flushed before every timed step (512 MB write)"},
+        "e2e": {"value": world * m_lower * e2e_steps / (e2e_total / 1e3), "unit": UNIT,
+                "h2d_bytes_per_step": 8 * m_in, "d2h_bytes_per_step": 8 + 24},
+        "gpu_launches": launches_per_step(n, tile, odeg, m_in) * args.steps,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": traffic,
+                     "kernel": f"k_count<{tile}>", "algorithmic_bytes": bytes_count,
+                     "kernel_ms": tc * 1e3, "peak_source": peak_src},
+        "phases": {"count_ms": tc * 1e3, "build_ms": tb * 1e3,
+                   "build_gbs": bytes_build / tb / 1e9,
+                   "count_edges_per_s": m_lower / tc},
+        "clocks": clk.summary(),
+    }
+
+    if rank == 0 and world == 1:
+        from oracle import oracle as O
+        try:
+            rp, col, _ = O.lower_csr(src, dst, n, "degree" if odeg else "natural")
+            if O.ref_cpu_available():
+                cnt, t, threads, reps_cpu = cpu_reference(rp, col, m_lower, args.cpu_budget)
+                assert cnt == expected, (cnt, expected)
+                line["cpu_baseline"] = {"value": m_lower / t, "unit": UNIT, "cores": threads,
+                                        "kind": "reference",
+                                        "sample": f"full graph, median of {reps_cpu} counts"}
+            if O.ref_gpu_available() and not args.no_ref_gpu:
+                rr, cc = rp_to_coo(rp, col)
+                ref = O.ref_gpu_run(rr, cc, n, tile, warmup=3, repeat=20)
+                assert ref["count"] == expected, (ref["count"], expected)
+                kms = statistics.median(ref["kernel_ms"])
+                line["reference_gpu"] = {
+                    "what": "reference convert + adaptive count compiled for sm_100a, same box",
+                    "convert_ms": ref["convert_ms"], "kernel_ms": kms,
+                    "engine_build_ms": tb * 1e3, "engine_count_ms_l2_flushed": tc * 1e3,
+                    "engine_count_ms_l2_warm": tc_warm,
+                    "count_speedup_same_l2_state": kms / tc_warm,
+                    "note": "reference kernel timed by its own events, L2 warm"}
+        except Exception as e:  # baselines are reported, never required
+            log("baseline leg failed:", repr(e))
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    g.free()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def rp_to_coo(rowptr, col):
+    rows = np.repeat(np.arange(len(rowptr) - 1, dtype=np.int32), np.diff(rowptr))
+    return rows, col
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,328 @@
+"""Python host mirror of the reference's Bit-BSR build + count interface.
+
+Names, argument meaning and call order follow fanna1234/btc-tc-artifact's
+``namespace btc`` (btc/btc.h):
+
+    coo = CooMatrix.from_edges(src, dst, n)                # btc/formats/coo.h
+    preprocess_for_triangle_counting(coo)                  # convert.h:600
+    bcsr = BCSR_16x128_Device()                            # bcsr_16x128.h:24
+    convert_coo_to_bcsr_16x128_gpu(bcsr, coo)              # bcsr_16x128.h:136
+    count = count_triangles_16x128_adaptive(bcsr, 2048)    # tc_16x128_adaptive.h:12
+    bcsr.free()
+
+Every call goes through libbtc_b200.so (include/btc_c.h).  Where the reference
+printed and returned on failure, these raise ``BtcError``.  Device arrays are
+torch CUDA int32 tensors (torch is only the allocator and stream provider here);
+host arrays are numpy.
+
+``BitBSR`` is the stream-ordered handle API (btc_build_bitbsr / btc_count).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import BtcError, check, lib
+
+__all__ = [
+    "BtcError", "CooMatrix", "BCSR_16x128_Device", "BCSR_16x32_Device",
+    "convert_coo_to_bcsr_16x128_gpu", "convert_coo_to_bcsr_16x32_gpu",
+    "count_triangles_16x128_adaptive", "count_triangles_16x32_adaptive",
+    "preprocess_for_triangle_counting", "lite_select_tile_cols", "BitBSR", "default_tau",
+]
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _stream_ptr(stream) -> int | None:
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    return int(stream.cuda_stream)
+
+
+# ---------------------------------------------------------------------------
+# reference-shaped surface
+# ---------------------------------------------------------------------------
+
+class CooMatrix:
+    """Device COO matrix (btc/formats/coo.h:10-33): int32 row/column index tensors."""
+
+    def __init__(self, row_indices, column_indices, num_rows: int, num_cols: int | None = None):
+        torch = _torch()
+        self.row_indices = torch.as_tensor(row_indices, dtype=torch.int32, device="cuda").contiguous()
+        self.column_indices = torch.as_tensor(column_indices, dtype=torch.int32,
+                                              device="cuda").contiguous()
+        self.num_rows = int(num_rows)
+        self.num_cols = int(num_cols if num_cols is not None else num_rows)
+
+    @classmethod
+    def from_edges(cls, src, dst, n: int) -> "CooMatrix":
+        return cls(src, dst, n)
+
+    @property
+    def num_entries(self) -> int:
+        return int(self.row_indices.numel())
+
+    def free(self):
+        torch = _torch()
+        self.row_indices = torch.zeros(0, dtype=torch.int32, device="cuda")
+        self.column_indices = torch.zeros(0, dtype=torch.int32, device="cuda")
+
+
+def preprocess_for_triangle_counting(coo: CooMatrix, force_cpu: bool = False,
+                                     lower_triangular: bool = True, input_file: str = "",
+                                     remap: bool = True) -> None:
+    """convert.h:600-612 with BTC_REORDER=0: orient to (max,min), drop self-loops,
+    sort, unique, and compact ids (remap).  Runs on the GPU whatever `force_cpu`
+    says (the engine has no CPU path); `lower_triangular=False` is not supported."""
+    if not lower_triangular:
+        raise BtcError(_lib.BTC_E_INVAL, "preprocess_for_triangle_counting(lower_triangular=False)")
+    nnz = C.c_int64(coo.num_entries)
+    rows = C.c_int32(coo.num_rows)
+    st = lib().btc_preprocess_for_triangle_counting(coo.row_indices.data_ptr(),
+                                                    coo.column_indices.data_ptr(),
+                                                    C.byref(nnz), C.byref(rows), int(remap))
+    check(st, "preprocess_for_triangle_counting")
+    coo.row_indices = coo.row_indices[: nnz.value].clone()
+    coo.column_indices = coo.column_indices[: nnz.value].clone()
+    coo.num_rows = coo.num_cols = int(rows.value)
+
+
+class _BcsrDevice:
+    TILE_COLS = 0
+    WORDS = 0
+
+    def __init__(self):
+        self._s = _lib.BtcBcsrDevice()
+
+    # reference fields
+    @property
+    def n(self): return self._s.n
+
+    @property
+    def n_row_blocks(self): return self._s.n_row_blocks
+
+    @property
+    def num_blocks(self): return self._s.num_blocks
+
+    @property
+    def indptr(self): return self._s.indptr
+
+    @property
+    def indices(self): return self._s.indices
+
+    @property
+    def row_indices(self): return self._s.row_indices
+
+    @property
+    def blocks(self): return self._s.blocks
+
+    @property
+    def result(self): return self._s.result
+
+    def free(self):
+        lib().btc_bcsr_free(C.byref(self._s))
+
+    def reset_result(self):
+        check(lib().btc_bcsr_reset_result(C.byref(self._s)), "reset_result")
+
+    def get_result(self) -> int:
+        v = C.c_ulonglong(0)
+        check(lib().btc_bcsr_get_result(C.byref(self._s), C.byref(v)), "get_result")
+        return int(v.value)
+
+    def to_host(self) -> dict:
+        """Copy the arrays out (for inspection and parity checks)."""
+        return _copy_out(self._s, self.TILE_COLS)
+
+    def __del__(self):
+        try:
+            if self._s.indptr:
+                self.free()
+        except Exception:
+            pass
+
+
+class BCSR_16x128_Device(_BcsrDevice):
+    TILE_COLS = 128
+
+
+class BCSR_16x32_Device(_BcsrDevice):
+    TILE_COLS = 32
+
+
+class _DeviceWords:
+    """Zero-copy view of `count` 32-bit words of engine-owned device memory."""
+
+    def __init__(self, ptr: int, count: int):
+        self.__cuda_array_interface__ = {"shape": (count,), "typestr": "<i4",
+                                         "data": (ptr, False), "version": 3}
+
+
+def _copy_out(s, tile_cols: int) -> dict:
+    torch = _torch()
+    tw = 16 * (tile_cols // 32)
+    B = int(s.num_blocks)
+    R = int(s.n_row_blocks)
+
+    def grab(ptr, count):
+        if count <= 0 or not ptr:
+            return np.zeros(max(count, 0), np.uint32)
+        view = _DeviceWords(int(ptr), int(count))
+        return torch.as_tensor(view, device="cuda").cpu().numpy().view(np.uint32).copy()
+
+    return dict(n=int(s.n), tile_cols=tile_cols, n_row_blocks=R, num_blocks=B,
+                indptr=grab(s.indptr, R + 1), indices=grab(s.indices, B),
+                row_indices=grab(s.row_indices, B), blocks=grab(s.blocks, B * tw))
+
+
+def _convert(fn, bcsr: _BcsrDevice, coo: CooMatrix):
+    if bcsr._s.indptr:
+        bcsr.free()
+    st = fn(C.byref(bcsr._s), coo.row_indices.data_ptr(), coo.column_indices.data_ptr(),
+            coo.num_entries, coo.num_rows)
+    check(st, fn.__name__)
+
+
+def convert_coo_to_bcsr_16x128_gpu(bcsr: BCSR_16x128_Device, coo: CooMatrix) -> None:
+    """bcsr_16x128.h:136-241."""
+    _convert(lib().btc_convert_coo_to_bcsr_16x128_gpu, bcsr, coo)
+
+
+def convert_coo_to_bcsr_16x32_gpu(bcsr: BCSR_16x32_Device, coo: CooMatrix) -> None:
+    """bcsr_16x32.h:144-249."""
+    _convert(lib().btc_convert_coo_to_bcsr_16x32_gpu, bcsr, coo)
+
+
+def _count(fn, bcsr: _BcsrDevice, threshold_blocks: int, kernel_ms):
+    out = C.c_ulonglong(0)
+    ms = C.c_float(0.0)
+    st = fn(C.byref(bcsr._s), int(threshold_blocks), C.byref(ms) if kernel_ms is not None else None,
+            C.byref(out))
+    check(st, fn.__name__)
+    if kernel_ms is not None:
+        kernel_ms.append(float(ms.value))
+    return int(out.value)
+
+
+def count_triangles_16x128_adaptive(bcsr: BCSR_16x128_Device, threshold_blocks: int = 2048,
+                                    kernel_ms: list | None = None) -> int:
+    """tc_16x128_adaptive.h:12-29.  `kernel_ms`, if a list, receives the kernel time."""
+    return _count(lib().btc_count_triangles_16x128_adaptive, bcsr, threshold_blocks, kernel_ms)
+
+
+def count_triangles_16x32_adaptive(bcsr: BCSR_16x32_Device, threshold_blocks: int = 40000,
+                                   kernel_ms: list | None = None) -> int:
+    """tc_16x32_adaptive.h:14-31."""
+    return _count(lib().btc_count_triangles_16x32_adaptive, bcsr, threshold_blocks, kernel_ms)
+
+
+def lite_select_tile_cols(nnz: int, num_rows: int, mode: int = 0) -> int:
+    """BTC-Lite O(1) policy (apps/btc_tc_lite.cu:45-65)."""
+    return int(lib().btc_lite_select_tile_cols(int(nnz), int(num_rows), int(mode)))
+
+
+def default_tau(tile_cols: int) -> int:
+    return int(lib().btc_default_tau(int(tile_cols)))
+
+
+# ---------------------------------------------------------------------------
+# stream-ordered handle API
+# ---------------------------------------------------------------------------
+
+def _edge_ptrs(src, dst):
+    """(src_ptr, dst_ptr, m, flags, keepalive) for torch CUDA tensors or numpy arrays."""
+    if isinstance(src, np.ndarray) or isinstance(dst, np.ndarray):
+        s = np.ascontiguousarray(src, dtype=np.int32)
+        d = np.ascontiguousarray(dst, dtype=np.int32)
+        if s.shape != d.shape:
+            raise BtcError(_lib.BTC_E_INVAL, "edge arrays differ in length")
+        return s.ctypes.data, d.ctypes.data, int(s.size), _lib.BTC_INPUT_ON_HOST, (s, d)
+    torch = _torch()
+    if src.dtype != torch.int32 or dst.dtype != torch.int32:
+        raise BtcError(_lib.BTC_E_INVAL, "edge tensors must be int32")
+    if src.numel() != dst.numel():
+        raise BtcError(_lib.BTC_E_INVAL, "edge arrays differ in length")
+    s = src.contiguous()
+    d = dst.contiguous()
+    flags = _lib.BTC_INPUT_ON_HOST if not s.is_cuda else 0
+    return s.data_ptr(), d.data_ptr(), int(s.numel()), flags, (s, d)
+
+
+class BitBSR:
+    """Device-resident Bit-BSR handle (btc_build_bitbsr ... btc_free)."""
+
+    def __init__(self, src, dst, n: int, tile_cols: int = 0, orient_degree: bool = False,
+                 stream=None):
+        self._h = C.c_void_p(None)
+        sp, dp, m, flags, self._keep = _edge_ptrs(src, dst)
+        if orient_degree:
+            flags |= _lib.BTC_ORIENT_DEGREE
+        st = lib().btc_build_bitbsr(sp, dp, m, int(n), int(tile_cols), flags, _stream_ptr(stream),
+                                    C.byref(self._h))
+        check(st, "btc_build_bitbsr")
+        self._keep = None
+
+    def rebuild(self, src, dst, n: int, tile_cols: int = 0, orient_degree: bool = False,
+                stream=None) -> None:
+        sp, dp, m, flags, keep = _edge_ptrs(src, dst)
+        if orient_degree:
+            flags |= _lib.BTC_ORIENT_DEGREE
+        check(lib().btc_rebuild_bitbsr(self._h, sp, dp, m, int(n), int(tile_cols), flags,
+                                       _stream_ptr(stream)), "btc_rebuild_bitbsr")
+        del keep
+
+    def count(self, tau: int = _lib.BTC_TAU_DEFAULT, stream=None, timing: bool = False):
+        out = C.c_ulonglong(0)
+        ms = C.c_float(0.0)
+        check(lib().btc_count(self._h, int(tau), _stream_ptr(stream), C.byref(out),
+                              C.byref(ms) if timing else None), "btc_count")
+        return (int(out.value), float(ms.value)) if timing else int(out.value)
+
+    def count_async(self, tau: int = _lib.BTC_TAU_DEFAULT, stream=None, d_out: int | None = None):
+        check(lib().btc_count_async(self._h, int(tau), _stream_ptr(stream), d_out), "btc_count_async")
+
+    def info(self) -> _lib.BtcBitbsrView:
+        v = _lib.BtcBitbsrView()
+        check(lib().btc_bitbsr_info(self._h, C.byref(v)), "btc_bitbsr_info")
+        return v
+
+    @property
+    def num_tiles(self) -> int:
+        return int(self.info().bcsr.num_blocks)
+
+    @property
+    def tile_cols(self) -> int:
+        return int(self.info().tile_cols)
+
+    @property
+    def num_edges(self) -> int:
+        return int(self.info().num_edges)
+
+    def density_hist(self, stream=None) -> np.ndarray:
+        tc = self.tile_cols
+        h = np.zeros(16 * tc + 1, np.uint64)
+        check(lib().btc_density_hist(self._h, _stream_ptr(stream), h.ctypes.data), "btc_density_hist")
+        return h
+
+    def to_host(self) -> dict:
+        v = self.info()
+        return _copy_out(v.bcsr, int(v.tile_cols))
+
+    def free(self) -> None:
+        if self._h:
+            lib().btc_free(self._h)
+            self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

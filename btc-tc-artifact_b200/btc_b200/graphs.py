@@ -1,0 +1,176 @@
+"""Seeded synthetic graph generators for the engine's workloads.
+
+Every generator returns ``(src, dst, n)``: two int32 arrays holding each
+undirected edge once (no self-loops, no duplicates), in a seeded random
+orientation and order, and the vertex count.  The engine's builder orients,
+deduplicates and tiles them itself, so the order carries no information.
+
+Workloads (sizes as used by bench.py):
+  * ``erdos_renyi(16384, 16, seed=1)``      G(n, m = n*d/2 draws), ~131k edges
+  * ``stencil27(64)``                      27-point 3-D stencil, 262,144 vertices,
+                                           3,298,428 edges, 11,049,696 triangles
+  * ``rmat(22, 16, seed=7)``               R-MAT (.57,.19,.19,.05), ~64M edges
+  * ``sbm(n, 8, p_in, 0.001, seed)``       8-community stochastic block model
+  * ``stencil7(k)``                        7-point stencil (bipartite: 0 triangles)
+  * ``complete(n)``                        K_n (C(n,3) triangles)
+
+The reference ships no inputs for these (its SuiteSparse files are absent), so
+seeded synthetic graphs with the stated shapes stand in for them.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def _finish(lo, hi, n, rng):
+    """Dedup undirected pairs (lo < hi), then shuffle order and orientation."""
+    key = np.unique(hi.astype(np.int64) * np.int64(n) + lo.astype(np.int64))
+    hi = (key // n).astype(np.int32)
+    lo = (key % n).astype(np.int32)
+    if rng is None:
+        return hi, lo, n
+    perm = rng.permutation(len(key))
+    hi, lo = hi[perm], lo[perm]
+    flip = rng.random(len(key)) < 0.5
+    src = np.where(flip, lo, hi).astype(np.int32)
+    dst = np.where(flip, hi, lo).astype(np.int32)
+    return src, dst, n
+
+
+def _pairs_to_edges(u, v, n, rng):
+    u = np.asarray(u, np.int64)
+    v = np.asarray(v, np.int64)
+    keep = u != v
+    u, v = u[keep], v[keep]
+    return _finish(np.minimum(u, v), np.maximum(u, v), n, rng)
+
+
+def erdos_renyi(n: int, mean_degree: float, seed: int = 1):
+    """G(n, m) with m = round(n * mean_degree / 2) uniform draws; self-loops and
+    duplicate pairs removed."""
+    rng = np.random.default_rng(seed)
+    m = int(round(n * mean_degree / 2))
+    u = rng.integers(0, n, m, dtype=np.int64)
+    v = rng.integers(0, n, m, dtype=np.int64)
+    return _pairs_to_edges(u, v, n, rng)
+
+
+def _stencil(k: int, offsets, seed):
+    idx = np.arange(k ** 3, dtype=np.int64)
+    x, y, z = idx // (k * k), (idx // k) % k, idx % k
+    us, vs = [], []
+    for dx, dy, dz in offsets:
+        ok = ((x + dx >= 0) & (x + dx < k) & (y + dy >= 0) & (y + dy < k)
+              & (z + dz >= 0) & (z + dz < k))
+        u = idx[ok]
+        us.append(u)
+        vs.append(u + dx * k * k + dy * k + dz)
+    u = np.concatenate(us)
+    v = np.concatenate(vs)
+    rng = np.random.default_rng(seed) if seed is not None else None
+    return _finish(np.minimum(u, v), np.maximum(u, v), k ** 3, rng)
+
+
+def stencil27(k: int, seed: int | None = 0):
+    """27-point stencil on a k^3 grid, vertex id x*k*k + y*k + z (natural
+    lexicographic order); every pair of distinct cells at Chebyshev distance 1."""
+    offs = [(dx, dy, dz) for dx in (-1, 0, 1) for dy in (-1, 0, 1) for dz in (-1, 0, 1)
+            if (dx, dy, dz) > (0, 0, 0)]
+    return _stencil(k, offs, seed)
+
+
+def stencil7(k: int, seed: int | None = 0):
+    """7-point stencil on a k^3 grid (bipartite, so it has no triangles)."""
+    return _stencil(k, [(1, 0, 0), (0, 1, 0), (0, 0, 1)], seed)
+
+
+def complete(n: int, seed: int | None = 0):
+    u, v = np.triu_indices(n, 1)
+    rng = np.random.default_rng(seed) if seed is not None else None
+    return _finish(u, v, n, rng)
+
+
+def rmat(scale: int, edge_factor: int, a=0.57, b=0.19, c=0.19, seed: int = 7,
+         degree_order: bool = False):
+    """R-MAT: edge_factor * 2^scale draws of recursive quadrant choices with
+    probabilities (a, b, c, 1-a-b-c); symmetrised, deduplicated, self-loops
+    removed.  degree_order=True relabels vertices by descending degree (ties by
+    id), so hubs get the lowest ids."""
+    rng = np.random.default_rng(seed)
+    n = 1 << scale
+    m = edge_factor << scale
+    u = np.zeros(m, np.int64)
+    v = np.zeros(m, np.int64)
+    chunk = 1 << 22
+    ab, abc = a + b, a + b + c
+    for s in range(0, m, chunk):
+        e = min(m, s + chunk)
+        uu = np.zeros(e - s, np.int64)
+        vv = np.zeros(e - s, np.int64)
+        for _ in range(scale):
+            r = rng.random(e - s, dtype=np.float32)
+            row = r >= ab
+            colb = ((r >= a) & (r < ab)) | (r >= abc)
+            uu = (uu << 1) | row
+            vv = (vv << 1) | colb
+        u[s:e] = uu
+        v[s:e] = vv
+    src, dst, n = _pairs_to_edges(u, v, n, rng)
+    if degree_order:
+        src, dst = relabel_by_degree(src, dst, n)
+    return src, dst, n
+
+
+def relabel_by_degree(src, dst, n):
+    """Relabel so that rank 0 has the highest degree (ties by lower id)."""
+    deg = np.bincount(src, minlength=n) + np.bincount(dst, minlength=n)
+    order = np.lexsort((np.arange(n), -deg))
+    rank = np.empty(n, np.int32)
+    rank[order] = np.arange(n, dtype=np.int32)
+    return rank[src], rank[dst]
+
+
+def sbm(n: int, blocks: int, p_in: float, p_out: float, seed: int = 0):
+    """Stochastic block model with `blocks` equal communities: each block pair
+    draws Binomial(pairs, p) uniform vertex pairs (duplicates then removed)."""
+    rng = np.random.default_rng(seed)
+    bounds = np.linspace(0, n, blocks + 1).astype(np.int64)
+    us, vs = [], []
+    for i in range(blocks):
+        for j in range(i, blocks):
+            ni = bounds[i + 1] - bounds[i]
+            nj = bounds[j + 1] - bounds[j]
+            pairs = ni * (ni - 1) // 2 if i == j else ni * nj
+            p = p_in if i == j else p_out
+            k = rng.binomial(pairs, p) if pairs > 0 else 0
+            if k == 0:
+                continue
+            us.append(rng.integers(bounds[i], bounds[i + 1], k))
+            vs.append(rng.integers(bounds[j], bounds[j + 1], k))
+    if not us:
+        return np.zeros(0, np.int32), np.zeros(0, np.int32), n
+    return _pairs_to_edges(np.concatenate(us), np.concatenate(vs), n, rng)
+
+
+def lower_coo(src, dst, n):
+    """Sorted unique lower-triangular COO (row > col) of an edge list, in numpy.
+    Used to feed the reference-shaped entry points that expect a preprocessed COO."""
+    src = np.asarray(src, np.int64)
+    dst = np.asarray(dst, np.int64)
+    keep = src != dst
+    r = np.maximum(src[keep], dst[keep])
+    c = np.minimum(src[keep], dst[keep])
+    key = np.unique(r * np.int64(max(n, 1)) + c)
+    return (key // max(n, 1)).astype(np.int32), (key % max(n, 1)).astype(np.int32)
+
+
+def write_bin_csr(path: str, rowptr, col, n: int):
+    """Write the reference's binary CSR file (btc/utils/io/read.h:255-299):
+    int32 nrow, ncol, nnz; int32 row_ptr[nrow+1]; int32 col[nnz]; float val[nnz]."""
+    rowptr = np.asarray(rowptr, np.int32)
+    col = np.asarray(col, np.int32)
+    with open(path, "wb") as f:
+        np.array([n, n, len(col)], np.int32).tofile(f)
+        rowptr.tofile(f)
+        col.tofile(f)
+        np.ones(len(col), np.float32).tofile(f)

@@ -1,0 +1,151 @@
+// common.cuh -- shared definitions for the engine's CUDA sources (sm_100a only).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+
+#include "btc_c.h"
+
+#if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ < 1000)
+#error "this engine is written for sm_100a (B200) only"
+#endif
+
+namespace btc200 {
+
+constexpr int kWarp = 32;
+constexpr unsigned kFull = 0xffffffffu;
+
+// Status propagation for host code: evaluate a CUDA call, map failure to BTC_E_CUDA
+// (or BTC_E_NOMEM for allocation failures) and return from the enclosing function.
+#define BTC_CUDA_TRY(expr)                                                      \
+    do {                                                                        \
+        cudaError_t _e = (expr);                                                \
+        if (_e != cudaSuccess) {                                                \
+            ::btc200::note_cuda_error(_e, #expr, __FILE__, __LINE__);           \
+            return _e == cudaErrorMemoryAllocation ? BTC_E_NOMEM : BTC_E_CUDA;  \
+        }                                                                       \
+    } while (0)
+
+#define BTC_TRY(expr)                 \
+    do {                              \
+        int _s = (expr);              \
+        if (_s != BTC_OK) return _s;  \
+    } while (0)
+
+void note_cuda_error(cudaError_t e, const char* what, const char* file, int line);
+
+__device__ __forceinline__ unsigned lanemask_lt()
+{
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+__host__ __device__ __forceinline__ int bit_length_u64(uint64_t x)
+{
+#ifdef __CUDA_ARCH__
+    return x ? 64 - __clzll((long long)x) : 0;
+#else
+    return x ? 64 - __builtin_clzll(x) : 0;
+#endif
+}
+
+__host__ __device__ __forceinline__ int log2_exact(int x)
+{
+    int k = 0;
+    while ((1 << k) < x) ++k;
+    return k;
+}
+
+// A grow-only device buffer.  reserve() keeps contents only when no reallocation
+// happens; callers treat it as scratch.
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    int reserve(size_t need)
+    {
+        if (need <= bytes && ptr) return BTC_OK;
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        if (need == 0) return BTC_OK;
+        size_t want = need + need / 8;  // headroom for slowly growing rebuilds
+        cudaError_t e = cudaMalloc(&ptr, want);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            e = cudaMalloc(&ptr, need);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                ptr = nullptr;
+                return BTC_E_NOMEM;
+            }
+            want = need;
+        }
+        bytes = want;
+        return BTC_OK;
+    }
+    void release()
+    {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    template <class T>
+    T* as() const { return static_cast<T*>(ptr); }
+};
+
+// ---------------------------------------------------------------------------
+// Sort (radix.cu)
+// ---------------------------------------------------------------------------
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per CTA tile
+constexpr int kRadixBits = 8;
+constexpr int kRadix = 1 << kRadixBits;
+
+inline size_t sort_tiles(size_t n) { return (n + kSortTile - 1) / kSortTile; }
+
+// Scratch words needed by radix_sort_u64 for up to n keys.
+size_t radix_scratch_words(size_t n);
+
+// Stable LSD sort of keys[0, *d_count) by bits [lo_bit, hi_bit).  d_count lives in
+// device memory (at most max_n); alt is a second buffer of max_n keys.  Returns the
+// buffer holding the sorted keys (keys or alt).
+uint64_t* radix_sort_u64(uint64_t* keys, uint64_t* alt, size_t max_n,
+                         const unsigned long long* d_count, int lo_bit, int hi_bit,
+                         uint32_t* scratch, cudaStream_t s, int* status);
+
+// ---------------------------------------------------------------------------
+// Build (build.cu)
+// ---------------------------------------------------------------------------
+struct BuildGeom {
+    int32_t n;
+    int tile_cols;      // C
+    int log2c;          // log2(C)
+    int payload_bits;   // 4 + log2(C): (row in tile, column in tile)
+    int cb_bits;        // bits of the column-block id
+    int t_bits;         // bits of the tile key (row block, column block)
+    int32_t n_row_blocks;
+    int64_t n_col_blocks;
+};
+BuildGeom make_geom(int32_t n, int tile_cols);
+
+// ---------------------------------------------------------------------------
+// Count (count.cu)
+// ---------------------------------------------------------------------------
+struct CountScratch {
+    unsigned long long* partials;  // one per CTA of the persistent grid
+    unsigned int* done;            // CTAs finished (reset to 0 by the last one)
+    unsigned long long* result;    // where the final count lands
+    unsigned long long* result2;   // optional second destination (nullable)
+};
+
+int count_grid_size(int tile_cols);
+int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
+                 const uint32_t* row_indices, const uint32_t* blocks, uint32_t num_tiles,
+                 int32_t n_row_blocks, int tau, CountScratch scr, cudaStream_t s);
+
+int device_sm_count();
+
+}  // namespace btc200

@@ -1,0 +1,186 @@
+/*
+ * btc_c.h -- C ABI of the B200 (sm_100a) exact triangle-counting engine.
+ *
+ * The engine computes the masked product L (.) (L L^T) on Bit-BSR tiles, the path
+ * of fanna1234/btc-tc-artifact's btc/btc.h (Bit-BSR build + hybrid count).  That
+ * surface is a set of C++ templates; this header restates it as plain C: pointers,
+ * sizes and status codes, no C++ or torch types.  Every entry point names the
+ * reference interface it replaces (paths within fanna1234/btc-tc-artifact).
+ *
+ * Status codes: every int-returning call returns BTC_OK (0) or a negative BTC_E_*.
+ * Streams: btc_stream_t is a cudaStream_t (NULL = legacy default stream).
+ * Threading: calls on distinct handles are independent; calls that share a handle
+ * must be ordered by the caller (one stream, or host synchronisation), because a
+ * handle owns its build workspace and its count scratch.
+ */
+#ifndef BTC_C_H
+#define BTC_C_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* btc_stream_t;
+
+#if defined(__GNUC__)
+#define BTC_API __attribute__((visibility("default")))
+#else
+#define BTC_API
+#endif
+
+#define BTC_OK 0
+#define BTC_E_INVAL (-1)   /* bad argument: null pointer, tile width, size limit */
+#define BTC_E_NOMEM (-2)   /* device or pinned-host allocation failed */
+#define BTC_E_CUDA (-3)    /* CUDA runtime error (launch, copy, sync) */
+#define BTC_E_TIMEOUT (-4) /* reserved: a bounded device wait gave up */
+#define BTC_E_RANGE (-5)   /* an input vertex id lies outside [0, n) */
+
+/* Build flags (btc_build_bitbsr, btc_rebuild_bitbsr, btc_convert_*). */
+#define BTC_INPUT_ON_HOST 0x1u /* src/dst are host pointers (pinned or pageable) */
+#define BTC_ORIENT_DEGREE 0x2u /* relabel vertices by descending degree (ties by id)
+                                  before orienting each edge to (max, min) */
+
+/* Default dense/sparse switch: a tile takes the binary tensor-core path when its
+ * popcount exceeds tau.  Pass BTC_TAU_DEFAULT to use the engine's value. */
+#define BTC_TAU_DEFAULT (-1)
+#define BTC_TAU_ALL_SPARSE 0x7fffffff
+
+/* ======================================================================== */
+/* Reference-shaped surface                                                  */
+/* ======================================================================== */
+
+/* Field order, types and bit layout of btc::BCSR_16x128_Device
+ * (btc/operations/bcsr_16x128.h:24-32) and btc::BCSR_16x32_Device
+ * (btc/operations/bcsr_16x32.h:109-117):
+ *   indptr[n_row_blocks+1]  tile offsets per 16-row block
+ *   indices[num_blocks]     column-block id of each tile, ascending within a row block
+ *   row_indices[num_blocks] row-block id of each tile
+ *   blocks[num_blocks*W]    tile bits, row-major, W = 64 (16x128) or 16 (16x32) words;
+ *                           bit b of word (r*W/16 + w) is column 32w+b of tile row r
+ *   result                  device uint64 that receives the count
+ * All arrays are device memory owned by the engine (free with btc_bcsr_free). */
+typedef struct btc_bcsr_device {
+    uint32_t* indptr;
+    uint32_t* indices;
+    uint32_t* blocks;
+    uint32_t* row_indices;
+    unsigned long long* result;
+    int n;
+    int n_row_blocks;
+    uint32_t num_blocks;
+} btc_bcsr_device;
+
+/* Replaces btc::convert_coo_to_bcsr_16x128_gpu (btc/operations/bcsr_16x128.h:136-241).
+ * d_rows/d_cols: device COO of nnz entries on num_rows vertices.  The reference
+ * expects the preprocessed lower triangle; this call orients, drops self-loops and
+ * deduplicates itself, so any symmetric or one-sided edge list gives the same tiles.
+ * Blocking (legacy default stream).  Returns BTC_OK or BTC_E_*. */
+BTC_API int btc_convert_coo_to_bcsr_16x128_gpu(btc_bcsr_device* bcsr, const int32_t* d_rows,
+                                       const int32_t* d_cols, int64_t nnz, int32_t num_rows);
+
+/* Replaces btc::convert_coo_to_bcsr_16x32_gpu (btc/operations/bcsr_16x32.h:144-249). */
+BTC_API int btc_convert_coo_to_bcsr_16x32_gpu(btc_bcsr_device* bcsr, const int32_t* d_rows,
+                                      const int32_t* d_cols, int64_t nnz, int32_t num_rows);
+
+/* Replaces btc::count_triangles_16x128_adaptive (btc/operations/tc_16x128_adaptive.h:12-29)
+ * and count_triangles_16x128_v5/_v4.  threshold_blocks selected the reference's v4/v5
+ * variant; the engine has one kernel and accepts the argument for signature parity.
+ * kernel_ms (nullable) receives the kernel-only event time.  The count is written to
+ * *out_count and to bcsr->result.  Blocking. */
+BTC_API int btc_count_triangles_16x128_adaptive(btc_bcsr_device* bcsr, int threshold_blocks,
+                                        float* kernel_ms, unsigned long long* out_count);
+
+/* Replaces btc::count_triangles_16x32_adaptive (btc/operations/tc_16x32_adaptive.h:14-31). */
+BTC_API int btc_count_triangles_16x32_adaptive(btc_bcsr_device* bcsr, int threshold_blocks,
+                                       float* kernel_ms, unsigned long long* out_count);
+
+/* Replaces BCSR_*_Device::free() (bcsr_16x128.h:34-42): releases every array and
+ * nulls the pointers.  Safe on a zeroed or already freed struct. */
+BTC_API void btc_bcsr_free(btc_bcsr_device* bcsr);
+
+/* Replaces BCSR_*_Device::reset_result() / get_result() (bcsr_16x128.h:44-50). */
+BTC_API int btc_bcsr_reset_result(btc_bcsr_device* bcsr);
+BTC_API int btc_bcsr_get_result(const btc_bcsr_device* bcsr, unsigned long long* out);
+
+/* Replaces btc::preprocess_for_triangle_counting (btc/operations/convert.h:600-612 with
+ * BTC_REORDER=0): in place on device COO arrays, orient every entry to (max, min),
+ * drop self-loops, sort lexicographically and drop duplicates; with remap != 0 also
+ * compact vertex ids to [0, n_used) in ascending order (convert.h:386-425).  *nnz and
+ * *num_rows are updated.  Blocking. */
+BTC_API int btc_preprocess_for_triangle_counting(int32_t* d_rows, int32_t* d_cols, int64_t* nnz,
+                                         int32_t* num_rows, int remap);
+
+/* The BTC-Lite O(1) tile policy (apps/btc_tc_lite.cu:45-65): returns 32 or 128.
+ * mode 1 forces 32, mode 2 forces 128 (the reference's BTC_MODE), 0 applies
+ * "avg degree nnz/rows < 15 or rows < 50000 -> 32, else 128". */
+BTC_API int btc_lite_select_tile_cols(int64_t nnz, int32_t num_rows, int mode);
+
+/* ======================================================================== */
+/* Stream-ordered engine surface                                             */
+/* ======================================================================== */
+
+typedef struct btc_bitbsr btc_bitbsr; /* opaque, device-resident, owns its buffers */
+
+typedef struct btc_bitbsr_view {
+    btc_bcsr_device bcsr; /* the arrays, in the reference layout */
+    int tile_cols;        /* 32 or 128 */
+    int device;           /* CUDA ordinal the handle lives on */
+    int64_t num_edges;    /* unique lower edges (r > c) after dedup */
+    int64_t input_edges;  /* edges handed to the build, self-loops included */
+    size_t device_bytes;  /* device memory held by the handle */
+} btc_bitbsr_view;
+
+/* Builds the Bit-BSR of an edge list (src[i], dst[i]), i < m, on n vertices with
+ * 16 x tile_cols tiles (tile_cols 32 or 128; 0 applies btc_lite_select_tile_cols).
+ * Orientation to (max, min), self-loop removal and deduplication happen on the GPU.
+ * With BTC_INPUT_ON_HOST the arrays are host memory and are copied on `stream`.
+ * Synchronises `stream` once (to size the tile arrays).  *out receives a new handle.
+ * Limits: n < 2^31, m <= 2^32 - 4096, tiles < 2^32.  Replaces the preprocess + convert pair
+ * (convert.h:600, bcsr_16x128.h:136 / bcsr_16x32.h:144). */
+BTC_API int btc_build_bitbsr(const int32_t* src, const int32_t* dst, int64_t m, int32_t n, int tile_cols,
+                     uint32_t flags, btc_stream_t stream, btc_bitbsr** out);
+
+/* Same as btc_build_bitbsr into an existing handle, reusing its device buffers
+ * when they are large enough (no allocation in steady state). */
+BTC_API int btc_rebuild_bitbsr(btc_bitbsr* g, const int32_t* src, const int32_t* dst, int64_t m,
+                       int32_t n, int tile_cols, uint32_t flags, btc_stream_t stream);
+
+/* Counts the triangles of a handle: enqueues the count on `stream`, waits, and
+ * writes *out_count.  tau: dense/sparse switch (BTC_TAU_DEFAULT for the engine's).
+ * kernel_ms (nullable): event time of the count kernel alone.  Replaces
+ * count_triangles_16x{128,32}_adaptive (tc_16x128_adaptive.h:12, tc_16x32_adaptive.h:14). */
+BTC_API int btc_count(btc_bitbsr* g, int tau, btc_stream_t stream, unsigned long long* out_count,
+              float* kernel_ms);
+
+/* Enqueues the count on `stream` without waiting; the uint64 count lands in device
+ * memory at d_out (nullable: then only in the handle's result slot) when the
+ * stream reaches it. */
+BTC_API int btc_count_async(btc_bitbsr* g, int tau, btc_stream_t stream, unsigned long long* d_out);
+
+/* Fills *v with the handle's arrays and sizes. */
+BTC_API int btc_bitbsr_info(const btc_bitbsr* g, btc_bitbsr_view* v);
+
+/* Tile popcount histogram: hist[p] = number of tiles with exactly p bits set,
+ * p in [0, 16*tile_cols] (hist holds 16*tile_cols+1 host uint64).  Blocking. */
+BTC_API int btc_density_hist(btc_bitbsr* g, btc_stream_t stream, uint64_t* hist);
+
+/* Releases the handle and every buffer it owns.  NULL is a no-op. */
+BTC_API void btc_free(btc_bitbsr* g);
+
+/* Default tau for a tile width (the value BTC_TAU_DEFAULT resolves to). */
+BTC_API int btc_default_tau(int tile_cols);
+
+/* Static text for a status code. */
+BTC_API const char* btc_strerror(int status);
+
+/* ABI version: (major << 16) | minor. */
+BTC_API int btc_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BTC_C_H */

@@ -1,0 +1,64 @@
+"""CPU tests of the seeded generators (inputs of every parity test and of the bench)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from btc_b200 import graphs as G
+
+
+def _check_simple(src, dst, n):
+    assert src.dtype == np.int32 and dst.dtype == np.int32
+    assert np.all(src != dst)
+    assert src.min() >= 0 and dst.min() >= 0 and max(src.max(), dst.max()) < n
+    lo, hi = np.minimum(src, dst).astype(np.int64), np.maximum(src, dst).astype(np.int64)
+    key = hi * n + lo
+    assert len(np.unique(key)) == len(key)
+
+
+@pytest.mark.parametrize("k,edges", [(2, 28), (4, 468), (64, 3_298_428)])
+def test_stencil27_sizes(k, edges):
+    src, dst, n = G.stencil27(k)
+    assert n == k ** 3 and len(src) == edges
+    _check_simple(src, dst, n)
+
+
+def test_stencil7_size():
+    src, dst, n = G.stencil7(8)
+    assert len(src) == 3 * 8 * 8 * 7
+    _check_simple(src, dst, n)
+
+
+def test_er_is_seeded_and_simple():
+    a = G.erdos_renyi(2000, 8, seed=3)
+    b = G.erdos_renyi(2000, 8, seed=3)
+    c = G.erdos_renyi(2000, 8, seed=4)
+    assert np.array_equal(a[0], b[0]) and not np.array_equal(a[0], c[0])
+    _check_simple(*a)
+
+
+def test_rmat_degree_order_puts_hubs_first():
+    src, dst, n = G.rmat(10, 8, seed=11, degree_order=True)
+    _check_simple(src, dst, n)
+    deg = np.bincount(src, minlength=n) + np.bincount(dst, minlength=n)
+    assert np.all(np.diff(deg) <= 0)
+
+
+def test_sbm_and_complete():
+    _check_simple(*G.sbm(800, 8, 0.2, 0.01, seed=1))
+    src, dst, n = G.complete(10)
+    assert len(src) == 45
+
+
+def test_lower_coo_and_bin_writer(tmp_path):
+    src = np.array([1, 0, 2, 2, 3], np.int32)
+    dst = np.array([0, 1, 1, 2, 0], np.int32)
+    r, c = G.lower_coo(src, dst, 4)
+    assert r.tolist() == [1, 2, 3] and c.tolist() == [0, 1, 0]
+    rowptr = np.array([0, 0, 1, 2, 3], np.int32)
+    p = tmp_path / "g.bin"
+    G.write_bin_csr(str(p), rowptr, c, 4)
+    raw = np.fromfile(p, np.int32)
+    assert raw[:3].tolist() == [4, 4, 3]
+    assert raw[3:8].tolist() == rowptr.tolist()
+    assert raw[8:11].tolist() == c.tolist()
