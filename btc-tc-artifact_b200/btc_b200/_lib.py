@@ -19,6 +19,7 @@ BTC_E_RANGE = -5
 
 BTC_INPUT_ON_HOST = 0x1
 BTC_ORIENT_DEGREE = 0x2
+BTC_BUILD_RADIX = 0x4
 BTC_TAU_DEFAULT = -1
 BTC_TAU_ALL_SPARSE = 0x7FFFFFFF
 

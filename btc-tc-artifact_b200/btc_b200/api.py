@@ -260,21 +260,25 @@ class BitBSR:
     """Device-resident Bit-BSR handle (btc_build_bitbsr ... btc_free)."""
 
     def __init__(self, src, dst, n: int, tile_cols: int = 0, orient_degree: bool = False,
-                 stream=None):
+                 stream=None, radix: bool = False):
         self._h = C.c_void_p(None)
         sp, dp, m, flags, self._keep = _edge_ptrs(src, dst)
         if orient_degree:
             flags |= _lib.BTC_ORIENT_DEGREE
+        if radix:
+            flags |= _lib.BTC_BUILD_RADIX
         st = lib().btc_build_bitbsr(sp, dp, m, int(n), int(tile_cols), flags, _stream_ptr(stream),
                                     C.byref(self._h))
         check(st, "btc_build_bitbsr")
         self._keep = None
 
     def rebuild(self, src, dst, n: int, tile_cols: int = 0, orient_degree: bool = False,
-                stream=None) -> None:
+                stream=None, radix: bool = False) -> None:
         sp, dp, m, flags, keep = _edge_ptrs(src, dst)
         if orient_degree:
             flags |= _lib.BTC_ORIENT_DEGREE
+        if radix:
+            flags |= _lib.BTC_BUILD_RADIX
         check(lib().btc_rebuild_bitbsr(self._h, sp, dp, m, int(n), int(tile_cols), flags,
                                        _stream_ptr(stream)), "btc_rebuild_bitbsr")
         del keep

@@ -1,0 +1,337 @@
+// bitmap.cu -- sort-free Bit-BSR builder.
+//
+// The tiles of L are the cells (row block rb, column block cb) that hold at least
+// one edge.  When the R x ceil(ncb/32) word grid of those cells is small enough, the
+// builder marks every edge's cell in a presence bitmap and numbers the tiles by a
+// popcount prefix over it; row-major cell order is exactly the reference's tile order
+// (indices ascending within a row block, row blocks ascending).  Then:
+//
+//   k_mark       one pass over the edges: orient (max,min), range-check, drop
+//                self-loops, set the cell bit (fire-and-forget atomicOr)
+//   k_bm_count   popcount per 4096-word chunk
+//   k_seg_scan   exclusive scan of the chunk counts -> chunk bases, tile total
+//   k_bm_emit    per word: exclusive tile prefix (kept for k_fill_bm), indices /
+//                row_indices of each set cell, indptr at row-block starts
+//   k_fill_bm    second pass over the edges: tile = prefix[word] + popc(lower bits of
+//                the word); OR the edge's bit into the tile
+//
+// Two reads of the edge list, one read and one write of the bitmap and its prefix
+// array, one write of the tiles: no sort.  Duplicate edges OR the same bit.
+#include "common.cuh"
+
+namespace btc200 {
+namespace bm {
+
+constexpr int kThreads = 256;
+constexpr int kWordsPerThread = 16;
+constexpr int kChunk = kThreads * kWordsPerThread;  // 4096 words per CTA
+
+__device__ __forceinline__ bool orient(int32_t u, int32_t v, int32_t n, const int32_t* rank,
+                                       uint32_t& r, uint32_t& c, bool& bad)
+{
+    bad = (u < 0) | (v < 0) | (u >= n) | (v >= n);
+    if (bad) return false;
+    if (rank) {
+        u = rank[u];
+        v = rank[v];
+    }
+    if (u == v) return false;
+    r = (uint32_t)max(u, v);
+    c = (uint32_t)min(u, v);
+    return true;
+}
+
+// Every cell bit is hit by all edges of its tile, so the word is read first and the
+// atomic is skipped when the bit is already set.  Bits only go from 0 to 1, so a
+// stale read can only cost a redundant atomic, never a missing one.
+template <int LOG2C>
+__global__ void __launch_bounds__(kThreads)
+k_mark(const int32_t* __restrict__ src, const int32_t* __restrict__ dst, int64_t m, int32_t n,
+       const int32_t* __restrict__ rank, uint64_t wpr, uint32_t* bitmap,
+       unsigned long long* __restrict__ bad_count)
+{
+    constexpr int U = 4;  // edges in flight per thread
+    uint32_t nbad = 0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < m; i0 += U * stride) {
+        int32_t u[U], v[U];
+#pragma unroll
+        for (int k = 0; k < U; ++k) {
+            const int64_t i = i0 + k * stride;
+            u[k] = i < m ? src[i] : 0;
+            v[k] = i < m ? dst[i] : 0;
+        }
+        uint64_t w[U];
+        uint32_t bit[U];
+        bool ok[U];
+#pragma unroll
+        for (int k = 0; k < U; ++k) {
+            uint32_t r = 0, c = 0;
+            bool bad = false;
+            ok[k] = (i0 + k * stride < m) && orient(u[k], v[k], n, rank, r, c, bad);
+            nbad += bad && (i0 + k * stride < m);
+            const uint32_t cb = c >> LOG2C;
+            w[k] = (uint64_t)(r >> 4) * wpr + (cb >> 5);
+            bit[k] = 1u << (cb & 31u);
+        }
+        uint32_t cur[U];
+#pragma unroll
+        for (int k = 0; k < U; ++k) cur[k] = ok[k] ? bitmap[w[k]] : 0xffffffffu;
+#pragma unroll
+        for (int k = 0; k < U; ++k)
+            if (!(cur[k] & bit[k])) atomicOr(&bitmap[w[k]], bit[k]);
+    }
+    nbad = __reduce_add_sync(kFull, nbad);
+    if ((threadIdx.x & 31) == 0 && nbad) atomicAdd(bad_count, (unsigned long long)nbad);
+}
+
+// Per-thread view of 16 consecutive bitmap words.
+__device__ __forceinline__ void load16(const uint32_t* __restrict__ bitmap, uint64_t w0, uint64_t W,
+                                       uint32_t (&x)[kWordsPerThread])
+{
+    if (w0 + kWordsPerThread <= W) {
+        const uint4* p = reinterpret_cast<const uint4*>(bitmap + w0);
+#pragma unroll
+        for (int q = 0; q < kWordsPerThread / 4; ++q) {
+            const uint4 v = p[q];
+            x[4 * q] = v.x;
+            x[4 * q + 1] = v.y;
+            x[4 * q + 2] = v.z;
+            x[4 * q + 3] = v.w;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < kWordsPerThread; ++k) x[k] = (w0 + k < W) ? bitmap[w0 + k] : 0u;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_bm_count(const uint32_t* __restrict__ bitmap, uint64_t W, uint32_t* __restrict__ chunk_count)
+{
+    __shared__ uint32_t s_warp[kThreads / kWarp];
+    const uint64_t w0 = (uint64_t)blockIdx.x * kChunk + (uint64_t)threadIdx.x * kWordsPerThread;
+    uint32_t x[kWordsPerThread];
+    load16(bitmap, w0, W, x);
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < kWordsPerThread; ++k) s += __popc(x[k]);
+    s = __reduce_add_sync(kFull, s);
+    if ((threadIdx.x & 31) == 0) s_warp[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < kThreads / kWarp; ++w) t += s_warp[w];
+        chunk_count[blockIdx.x] = t;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_bm_emit(const uint32_t* __restrict__ bitmap, uint64_t W, uint64_t wpr,
+          const uint32_t* __restrict__ chunk_base, uint32_t* __restrict__ prefix,
+          uint32_t* __restrict__ indices, uint32_t* __restrict__ row_indices,
+          uint32_t* __restrict__ indptr)
+{
+    __shared__ uint32_t s_warp[kThreads / kWarp];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t w0 = (uint64_t)blockIdx.x * kChunk + (uint64_t)threadIdx.x * kWordsPerThread;
+    uint32_t x[kWordsPerThread];
+    load16(bitmap, w0, W, x);
+    uint32_t mine = 0;
+#pragma unroll
+    for (int k = 0; k < kWordsPerThread; ++k) mine += __popc(x[k]);
+    // exclusive prefix of `mine` over the CTA (thread order = word order)
+    uint32_t incl = mine;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t t = __shfl_up_sync(kFull, incl, d);
+        if (lane >= d) incl += t;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    uint32_t base = chunk_base[blockIdx.x] + incl - mine;
+#pragma unroll
+    for (int w = 0; w < kThreads / kWarp; ++w) base += (w < warp) ? s_warp[w] : 0u;
+    if (w0 >= W) return;
+
+    uint64_t rb = w0 / wpr;
+    uint64_t col_word = w0 - rb * wpr;
+    uint32_t pre[kWordsPerThread];
+#pragma unroll
+    for (int k = 0; k < kWordsPerThread; ++k) {
+        pre[k] = base;
+        if (w0 + k < W) {
+            if (col_word == 0) indptr[rb] = base;
+            uint32_t bits = x[k];
+            uint32_t t = base;
+            while (bits) {
+                const int b = __ffs(bits) - 1;
+                bits &= bits - 1;
+                indices[t] = (uint32_t)(col_word * 32 + b);
+                row_indices[t] = (uint32_t)rb;
+                ++t;
+            }
+            base = t;
+        }
+        if (++col_word == wpr) {
+            col_word = 0;
+            ++rb;
+        }
+    }
+    if (w0 + kWordsPerThread <= W) {
+        uint4* p = reinterpret_cast<uint4*>(prefix + w0);
+#pragma unroll
+        for (int q = 0; q < kWordsPerThread / 4; ++q)
+            p[q] = make_uint4(pre[4 * q], pre[4 * q + 1], pre[4 * q + 2], pre[4 * q + 3]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < kWordsPerThread; ++k)
+            if (w0 + k < W) prefix[w0 + k] = pre[k];
+    }
+}
+
+template <int LOG2C>
+__global__ void __launch_bounds__(kThreads)
+k_fill_bm(const int32_t* __restrict__ src, const int32_t* __restrict__ dst, int64_t m, int32_t n,
+          const int32_t* __restrict__ rank, uint64_t wpr, const uint32_t* __restrict__ bitmap,
+          const uint32_t* __restrict__ prefix, uint32_t* __restrict__ blocks)
+{
+    constexpr int C = 1 << LOG2C;
+    constexpr int WPR = C / 32;
+    constexpr int TW = 16 * WPR;
+    constexpr int U = 4;  // edges in flight per thread
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < m; i0 += U * stride) {
+        int32_t u[U], v[U];
+#pragma unroll
+        for (int k = 0; k < U; ++k) {
+            const int64_t i = i0 + k * stride;
+            u[k] = i < m ? src[i] : 0;
+            v[k] = i < m ? dst[i] : 0;
+        }
+        uint32_t r[U], c[U];
+        bool ok[U];
+#pragma unroll
+        for (int k = 0; k < U; ++k) {
+            bool bad;
+            r[k] = c[k] = 0;
+            ok[k] = (i0 + k * stride < m) && orient(u[k], v[k], n, rank, r[k], c[k], bad);
+        }
+        uint32_t pre[U], word[U];
+#pragma unroll
+        for (int k = 0; k < U; ++k) {
+            const uint64_t w = (uint64_t)(r[k] >> 4) * wpr + ((c[k] >> LOG2C) >> 5);
+            pre[k] = ok[k] ? prefix[w] : 0u;
+            word[k] = ok[k] ? bitmap[w] : 0u;
+        }
+#pragma unroll
+        for (int k = 0; k < U; ++k) {
+            if (!ok[k]) continue;
+            const uint32_t below = (1u << ((c[k] >> LOG2C) & 31u)) - 1u;
+            const uint32_t t = pre[k] + __popc(word[k] & below);
+            const uint32_t cl = c[k] & (C - 1);
+            atomicOr(&blocks[(size_t)t * TW + (r[k] & 15u) * WPR + (cl >> 5)], 1u << (cl & 31u));
+        }
+    }
+}
+
+__global__ void k_set_last(uint32_t* __restrict__ indptr, int32_t R,
+                           const unsigned long long* __restrict__ total)
+{
+    indptr[R] = (uint32_t)*total;
+}
+
+template <int TW>
+__global__ void k_popcount_sum(const uint32_t* __restrict__ blocks, uint64_t words,
+                               unsigned long long* __restrict__ out)
+{
+    unsigned long long s = 0;
+    for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4; i < words;
+         i += (uint64_t)gridDim.x * blockDim.x * 4) {
+        const uint4 v = *reinterpret_cast<const uint4*>(blocks + i);
+        s += __popc(v.x) + __popc(v.y) + __popc(v.z) + __popc(v.w);
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) s += __shfl_down_sync(kFull, s, d);
+    if ((threadIdx.x & 31) == 0 && s) atomicAdd(out, s);
+}
+
+}  // namespace bm
+
+int grid_for(int64_t work, int threads);
+int launch_tile_scan(uint32_t* per_tile, uint32_t ntiles, unsigned long long* total, cudaStream_t s);
+
+static int edge_grid(int64_t m) { return grid_for((m + 15) / 16, bm::kThreads); }
+
+uint64_t bitmap_words_per_row(const BuildGeom& g)
+{
+    return (uint64_t)((g.n_col_blocks + 31) / 32);
+}
+
+size_t bitmap_chunks(uint64_t W) { return (size_t)((W + bm::kChunk - 1) / bm::kChunk); }
+
+int bitmap_mark_and_count(const BuildGeom& g, const int32_t* src, const int32_t* dst, int64_t m,
+                          const int32_t* rank, uint32_t* bitmap, uint32_t* chunk_count,
+                          unsigned long long* meta_bad, unsigned long long* meta_tiles,
+                          cudaStream_t s)
+{
+    const uint64_t wpr = bitmap_words_per_row(g);
+    const uint64_t W = wpr * (uint64_t)g.n_row_blocks;
+    if (W == 0) {
+        return cudaMemsetAsync(meta_tiles, 0, sizeof(unsigned long long), s) == cudaSuccess
+                   ? BTC_OK
+                   : BTC_E_CUDA;
+    }
+    if (cudaMemsetAsync(bitmap, 0, sizeof(uint32_t) * W, s) != cudaSuccess) return BTC_E_CUDA;
+    if (m > 0) {
+        if (g.tile_cols == 128)
+            bm::k_mark<7><<<edge_grid(m), bm::kThreads, 0, s>>>(src, dst, m, g.n, rank, wpr, bitmap,
+                                                                 meta_bad);
+        else
+            bm::k_mark<5><<<edge_grid(m), bm::kThreads, 0, s>>>(src, dst, m, g.n, rank, wpr, bitmap,
+                                                                 meta_bad);
+    }
+    const size_t chunks = bitmap_chunks(W);
+    bm::k_bm_count<<<(unsigned)chunks, bm::kThreads, 0, s>>>(bitmap, W, chunk_count);
+    if (cudaGetLastError() != cudaSuccess) return BTC_E_CUDA;
+    return launch_tile_scan(chunk_count, (uint32_t)chunks, meta_tiles, s);
+}
+
+int bitmap_emit_and_fill(const BuildGeom& g, const int32_t* src, const int32_t* dst, int64_t m,
+                         const int32_t* rank, const uint32_t* bitmap, const uint32_t* chunk_base,
+                         uint32_t* prefix, uint32_t* indices, uint32_t* row_indices,
+                         uint32_t* indptr, uint32_t* blocks, const unsigned long long* meta_tiles,
+                         cudaStream_t s)
+{
+    const uint64_t wpr = bitmap_words_per_row(g);
+    const uint64_t W = wpr * (uint64_t)g.n_row_blocks;
+    if (W > 0)
+        bm::k_bm_emit<<<(unsigned)bitmap_chunks(W), bm::kThreads, 0, s>>>(
+            bitmap, W, wpr, chunk_base, prefix, indices, row_indices, indptr);
+    bm::k_set_last<<<1, 1, 0, s>>>(indptr, g.n_row_blocks, meta_tiles);
+    if (m > 0 && W > 0) {
+        if (g.tile_cols == 128)
+            bm::k_fill_bm<7><<<edge_grid(m), bm::kThreads, 0, s>>>(src, dst, m, g.n, rank, wpr,
+                                                                    bitmap, prefix, blocks);
+        else
+            bm::k_fill_bm<5><<<edge_grid(m), bm::kThreads, 0, s>>>(src, dst, m, g.n, rank, wpr,
+                                                                    bitmap, prefix, blocks);
+    }
+    return cudaGetLastError() == cudaSuccess ? BTC_OK : BTC_E_CUDA;
+}
+
+int launch_popcount_sum(int tile_cols, const uint32_t* blocks, uint64_t num_tiles,
+                        unsigned long long* out, cudaStream_t s)
+{
+    const uint64_t words = num_tiles * (uint64_t)(16 * (tile_cols / 32));
+    if (cudaMemsetAsync(out, 0, sizeof(unsigned long long), s) != cudaSuccess) return BTC_E_CUDA;
+    if (words) {
+        const int grid = grid_for((int64_t)((words + 3) / 4), 256);
+        if (tile_cols == 128)
+            bm::k_popcount_sum<64><<<grid, 256, 0, s>>>(blocks, words, out);
+        else
+            bm::k_popcount_sum<16><<<grid, 256, 0, s>>>(blocks, words, out);
+    }
+    return cudaGetLastError() == cudaSuccess ? BTC_OK : BTC_E_CUDA;
+}
+
+}  // namespace btc200

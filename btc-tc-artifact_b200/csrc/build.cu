@@ -9,8 +9,7 @@
 //   k_seg_count      tile heads per sort tile
 //   k_seg_scan       exclusive scan of the head counts -> tile bases, tile total
 //   k_fill           tile ids from the head prefix; heads write indices/row_indices;
-//                    every edge ORs its bit into its tile (the atomicOr's old value
-//                    tells whether the edge is new, which counts unique edges)
+//                    every edge ORs its bit into its tile (duplicates OR the same bit)
 //   k_indptr         indptr[r] = lower_bound(row_indices, r)
 //   k_density        tile popcount histogram
 #include "common.cuh"
@@ -218,8 +217,7 @@ template <int LOG2C>
 __global__ void __launch_bounds__(kThreads)
 k_fill(const uint64_t* __restrict__ keys, const unsigned long long* __restrict__ d_count,
        int cb_bits, const uint32_t* __restrict__ tile_base, uint32_t* __restrict__ indices,
-       uint32_t* __restrict__ row_indices, uint32_t* __restrict__ blocks,
-       unsigned long long* __restrict__ uniq)
+       uint32_t* __restrict__ row_indices, uint32_t* __restrict__ blocks)
 {
     constexpr int C = 1 << LOG2C;
     constexpr int WPR = C / 32;
@@ -253,7 +251,6 @@ k_fill(const uint64_t* __restrict__ keys, const unsigned long long* __restrict__
 #pragma unroll
     for (int w = 0; w < kWarps; ++w) before += (w < warp) ? s_warp[w] : 0u;
 
-    uint32_t fresh = 0;
     const uint64_t cb_mask = (1ull << cb_bits) - 1ull;
 #pragma unroll
     for (int it = 0; it < kItems; ++it) {
@@ -270,14 +267,10 @@ k_fill(const uint64_t* __restrict__ keys, const unsigned long long* __restrict__
             }
             const uint32_t lr = (uint32_t)(k >> LOG2C) & 15u;
             const uint32_t cl = (uint32_t)k & (C - 1);
-            const uint32_t bit = 1u << (cl & 31u);
-            const uint32_t old = atomicOr(&blocks[(size_t)t * TW + lr * WPR + (cl >> 5)], bit);
-            fresh += (old & bit) ? 0u : 1u;
+            atomicOr(&blocks[(size_t)t * TW + lr * WPR + (cl >> 5)], 1u << (cl & 31u));
         }
         before += __popc(h);
     }
-    fresh = warp_sum(fresh);
-    if (lane == 0 && fresh) atomicAdd(uniq, (unsigned long long)fresh);
 }
 
 __global__ void k_indptr(const uint32_t* __restrict__ row_indices, uint32_t num_tiles,
@@ -385,16 +378,16 @@ int launch_segment(const BuildGeom& g, const uint64_t* keys, size_t max_n,
 
 int launch_fill(const BuildGeom& g, const uint64_t* keys, size_t max_n,
                 const unsigned long long* d_count, const uint32_t* tile_base, uint32_t* indices,
-                uint32_t* row_indices, uint32_t* blocks, unsigned long long* uniq, cudaStream_t s)
+                uint32_t* row_indices, uint32_t* blocks, cudaStream_t s)
 {
     const size_t tiles = sort_tiles(max_n);
     if (tiles > 0) {
         if (g.tile_cols == 128)
             build_kernels::k_fill<7><<<(unsigned)tiles, build_kernels::kThreads, 0, s>>>(
-                keys, d_count, g.cb_bits, tile_base, indices, row_indices, blocks, uniq);
+                keys, d_count, g.cb_bits, tile_base, indices, row_indices, blocks);
         else
             build_kernels::k_fill<5><<<(unsigned)tiles, build_kernels::kThreads, 0, s>>>(
-                keys, d_count, g.cb_bits, tile_base, indices, row_indices, blocks, uniq);
+                keys, d_count, g.cb_bits, tile_base, indices, row_indices, blocks);
     }
     return cudaGetLastError() == cudaSuccess ? BTC_OK : BTC_E_CUDA;
 }

@@ -19,7 +19,15 @@ int launch_make_keys(const BuildGeom&, const int32_t*, const int32_t*, int64_t, 
 int launch_segment(const BuildGeom&, const uint64_t*, size_t, const unsigned long long*, uint32_t*,
                    unsigned long long*, cudaStream_t);
 int launch_fill(const BuildGeom&, const uint64_t*, size_t, const unsigned long long*,
-                const uint32_t*, uint32_t*, uint32_t*, uint32_t*, unsigned long long*, cudaStream_t);
+                const uint32_t*, uint32_t*, uint32_t*, uint32_t*, cudaStream_t);
+uint64_t bitmap_words_per_row(const BuildGeom&);
+size_t bitmap_chunks(uint64_t W);
+int bitmap_mark_and_count(const BuildGeom&, const int32_t*, const int32_t*, int64_t, const int32_t*,
+                          uint32_t*, uint32_t*, unsigned long long*, unsigned long long*, cudaStream_t);
+int bitmap_emit_and_fill(const BuildGeom&, const int32_t*, const int32_t*, int64_t, const int32_t*,
+                         const uint32_t*, const uint32_t*, uint32_t*, uint32_t*, uint32_t*, uint32_t*,
+                         uint32_t*, const unsigned long long*, cudaStream_t);
+int launch_popcount_sum(int, const uint32_t*, uint64_t, unsigned long long*, cudaStream_t);
 int launch_indptr(const uint32_t*, uint32_t, int32_t, uint32_t*, cudaStream_t);
 int launch_density(int, const uint32_t*, uint32_t, unsigned long long*, cudaStream_t);
 int launch_set_u64(unsigned long long* p, unsigned long long v, cudaStream_t s);
@@ -66,7 +74,8 @@ struct btc_bitbsr {
     // Bit-BSR arrays (reference layout)
     DevBuf indptr, indices, row_indices, blocks, result;
     // build workspace
-    DevBuf in_src, in_dst, keys0, keys1, sort_scratch, tile_base, meta, deg, rank;
+    DevBuf in_src, in_dst, keys0, keys1, sort_scratch, tile_base, meta, deg, rank, bitmap, prefix;
+    bool used_bitmap = false;
     // count scratch
     DevBuf partials, done;
     unsigned long long* h_meta = nullptr;  // pinned, 8 slots
@@ -77,7 +86,7 @@ struct btc_bitbsr {
     {
         const DevBuf* all[] = {&indptr, &indices, &row_indices, &blocks, &result, &in_src, &in_dst,
                                &keys0, &keys1, &sort_scratch, &tile_base, &meta, &deg, &rank,
-                               &partials, &done};
+                               &bitmap, &prefix, &partials, &done};
         size_t s = 0;
         for (const DevBuf* b : all) s += b->bytes;
         return s;
@@ -86,7 +95,7 @@ struct btc_bitbsr {
     {
         DevBuf* all[] = {&indptr, &indices, &row_indices, &blocks, &result, &in_src, &in_dst,
                          &keys0, &keys1, &sort_scratch, &tile_base, &meta, &deg, &rank,
-                         &partials, &done};
+                         &bitmap, &prefix, &partials, &done};
         for (DevBuf* b : all) b->release();
         if (h_meta) cudaFreeHost(h_meta);
         h_meta = nullptr;
@@ -119,7 +128,7 @@ static int build_into(btc_bitbsr* g, const int32_t* src, const int32_t* dst, int
 {
     if (n < 0 || m < 0 || (uint64_t)m > kMaxEdges) return BTC_E_INVAL;
     if (m > 0 && (!src || !dst)) return BTC_E_INVAL;
-    if (flags & ~(BTC_INPUT_ON_HOST | BTC_ORIENT_DEGREE)) return BTC_E_INVAL;
+    if (flags & ~(BTC_INPUT_ON_HOST | BTC_ORIENT_DEGREE | BTC_BUILD_RADIX)) return BTC_E_INVAL;
     if (tile_cols == 0) tile_cols = btc_lite_select_tile_cols(m, n, 0);
     if (tile_cols != 32 && tile_cols != 128) return BTC_E_INVAL;
     BTC_CUDA_TRY(cudaGetDevice(&g->device));
@@ -158,18 +167,33 @@ static int build_into(btc_bitbsr* g, const int32_t* src, const int32_t* dst, int
         d_dst = g->in_dst.as<int32_t>();
     }
 
-    const size_t key_cap = (size_t)((flags & BTC_ORIENT_DEGREE) && n > m ? n : m);
-    BTC_TRY(g->keys0.reserve(sizeof(uint64_t) * (key_cap ? key_cap : 1)));
-    BTC_TRY(g->keys1.reserve(sizeof(uint64_t) * (key_cap ? key_cap : 1)));
-    BTC_TRY(g->sort_scratch.reserve(sizeof(uint32_t) * radix_scratch_words(key_cap)));
-    BTC_TRY(g->tile_base.reserve(sizeof(uint32_t) * (sort_tiles((size_t)m) + 1)));
+    // The cell bitmap (one bit per (row block, column block)) replaces the sort when it
+    // is small next to the edge list; otherwise the radix path sorts tile keys.
+    const uint64_t wpr = bitmap_words_per_row(geom);
+    const uint64_t bm_words = wpr * (uint64_t)geom.n_row_blocks;
+    const uint64_t bm_bytes = 4 * bm_words;
+    const bool use_bitmap = !(flags & BTC_BUILD_RADIX) && bm_bytes <= (4ull << 30) &&
+                            bm_bytes <= 32ull * (uint64_t)m + (64ull << 20);
+    g->used_bitmap = use_bitmap;
+
+    const bool degree = (flags & BTC_ORIENT_DEGREE) && n > 0;
+    size_t key_cap = use_bitmap ? 0 : (size_t)m;
+    if (degree && (size_t)n > key_cap) key_cap = (size_t)n;
+    if (key_cap) {
+        BTC_TRY(g->keys0.reserve(sizeof(uint64_t) * key_cap));
+        BTC_TRY(g->keys1.reserve(sizeof(uint64_t) * key_cap));
+        BTC_TRY(g->sort_scratch.reserve(sizeof(uint32_t) * radix_scratch_words(key_cap)));
+    }
+    const size_t chunk_slots =
+        use_bitmap ? bitmap_chunks(bm_words) : sort_tiles((size_t)m);
+    BTC_TRY(g->tile_base.reserve(sizeof(uint32_t) * (chunk_slots + 1)));
     uint64_t* k0 = g->keys0.as<uint64_t>();
     uint64_t* k1 = g->keys1.as<uint64_t>();
     int st = BTC_OK;
 
     // ---- optional descending-degree relabel ---------------------------------
     const int32_t* rank = nullptr;
-    if ((flags & BTC_ORIENT_DEGREE) && n > 0) {
+    if (degree) {
         BTC_TRY(g->deg.reserve(sizeof(uint32_t) * (size_t)n));
         BTC_TRY(g->rank.reserve(sizeof(int32_t) * (size_t)n));
         BTC_CUDA_TRY(cudaMemsetAsync(g->deg.ptr, 0, sizeof(uint32_t) * (size_t)n, s));
@@ -186,14 +210,24 @@ static int build_into(btc_bitbsr* g, const int32_t* src, const int32_t* dst, int
         rank = g->rank.as<int32_t>();
     }
 
-    // ---- keys, sort, segmentation -------------------------------------------
-    BTC_TRY(launch_make_keys(geom, d_src, d_dst, m, rank, k0, meta, s));
-    uint64_t* sorted = radix_sort_u64(k0, k1, (size_t)m, meta + kMetaValid, geom.payload_bits,
-                                      geom.payload_bits + geom.t_bits,
-                                      g->sort_scratch.as<uint32_t>(), s, &st);
-    BTC_TRY(st);
-    BTC_TRY(launch_segment(geom, sorted, (size_t)m, meta + kMetaValid, g->tile_base.as<uint32_t>(),
-                           meta + kMetaTiles, s));
+    const size_t TW = (size_t)16 * (tile_cols / 32);
+    uint64_t* sorted = nullptr;
+    if (use_bitmap) {
+        BTC_TRY(g->bitmap.reserve(sizeof(uint32_t) * (bm_words ? bm_words : 1)));
+        BTC_TRY(g->prefix.reserve(sizeof(uint32_t) * (bm_words ? bm_words : 1)));
+        BTC_TRY(bitmap_mark_and_count(geom, d_src, d_dst, m, rank, g->bitmap.as<uint32_t>(),
+                                      g->tile_base.as<uint32_t>(), meta + kMetaBad,
+                                      meta + kMetaTiles, s));
+    } else {
+        // ---- keys, sort, segmentation ---------------------------------------
+        BTC_TRY(launch_make_keys(geom, d_src, d_dst, m, rank, k0, meta, s));
+        sorted = radix_sort_u64(k0, k1, (size_t)m, meta + kMetaValid, geom.payload_bits,
+                                geom.payload_bits + geom.t_bits, g->sort_scratch.as<uint32_t>(), s,
+                                &st);
+        BTC_TRY(st);
+        BTC_TRY(launch_segment(geom, sorted, (size_t)m, meta + kMetaValid,
+                               g->tile_base.as<uint32_t>(), meta + kMetaTiles, s));
+    }
     BTC_CUDA_TRY(cudaMemcpyAsync(g->h_meta, meta, sizeof(unsigned long long) * 3,
                                  cudaMemcpyDeviceToHost, s));
     BTC_CUDA_TRY(cudaStreamSynchronize(s));
@@ -203,7 +237,6 @@ static int build_into(btc_bitbsr* g, const int32_t* src, const int32_t* dst, int
     g->num_tiles = (uint32_t)tiles;
 
     // ---- tile arrays ----------------------------------------------------------
-    const size_t TW = (size_t)16 * (tile_cols / 32);
     BTC_TRY(g->indptr.reserve(sizeof(uint32_t) * ((size_t)geom.n_row_blocks + 1)));
     BTC_TRY(g->indices.reserve(sizeof(uint32_t) * (tiles ? tiles : 1)));
     BTC_TRY(g->row_indices.reserve(sizeof(uint32_t) * (tiles ? tiles : 1)));
@@ -211,11 +244,19 @@ static int build_into(btc_bitbsr* g, const int32_t* src, const int32_t* dst, int
     BTC_TRY(ensure_count_scratch(g));
     if (tiles)
         BTC_CUDA_TRY(cudaMemsetAsync(g->blocks.ptr, 0, sizeof(uint32_t) * TW * tiles, s));
-    BTC_TRY(launch_fill(geom, sorted, (size_t)m, meta + kMetaValid, g->tile_base.as<uint32_t>(),
-                        g->indices.as<uint32_t>(), g->row_indices.as<uint32_t>(),
-                        g->blocks.as<uint32_t>(), meta + kMetaUniq, s));
-    BTC_TRY(launch_indptr(g->row_indices.as<uint32_t>(), g->num_tiles, geom.n_row_blocks,
-                          g->indptr.as<uint32_t>(), s));
+    if (use_bitmap) {
+        BTC_TRY(bitmap_emit_and_fill(geom, d_src, d_dst, m, rank, g->bitmap.as<uint32_t>(),
+                                     g->tile_base.as<uint32_t>(), g->prefix.as<uint32_t>(),
+                                     g->indices.as<uint32_t>(), g->row_indices.as<uint32_t>(),
+                                     g->indptr.as<uint32_t>(), g->blocks.as<uint32_t>(),
+                                     meta + kMetaTiles, s));
+    } else {
+        BTC_TRY(launch_fill(geom, sorted, (size_t)m, meta + kMetaValid, g->tile_base.as<uint32_t>(),
+                            g->indices.as<uint32_t>(), g->row_indices.as<uint32_t>(),
+                            g->blocks.as<uint32_t>(), s));
+        BTC_TRY(launch_indptr(g->row_indices.as<uint32_t>(), g->num_tiles, geom.n_row_blocks,
+                              g->indptr.as<uint32_t>(), s));
+    }
     return BTC_OK;
 }
 
@@ -322,9 +363,11 @@ int btc_bitbsr_info(const btc_bitbsr* gc, btc_bitbsr_view* v)
     if (!gc || !v) return BTC_E_INVAL;
     btc_bitbsr* g = const_cast<btc_bitbsr*>(gc);
     if (!g->edges_known) {
+        // unique lower edges = bits set in the tiles (duplicates OR the same bit)
         unsigned long long u = 0;
-        BTC_CUDA_TRY(cudaMemcpy(&u, g->meta.as<unsigned long long>() + kMetaUniq, sizeof(u),
-                                cudaMemcpyDeviceToHost));
+        unsigned long long* d = g->meta.as<unsigned long long>() + kMetaUniq;
+        BTC_TRY(launch_popcount_sum(g->tile_cols, g->blocks.as<uint32_t>(), g->num_tiles, d, nullptr));
+        BTC_CUDA_TRY(cudaMemcpy(&u, d, sizeof(u), cudaMemcpyDeviceToHost));
         g->num_edges = (int64_t)u;
         g->edges_known = true;
     }

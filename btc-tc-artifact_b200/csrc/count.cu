@@ -40,17 +40,19 @@ struct Cfg {
     static constexpr int MAXBITS = 16 * C;   // bits per tile
 };
 
+constexpr int kMCap = 64;   // matches buffered per warp before a bit pass
+constexpr int kBCap = 512;  // mask-bit codes buffered per warp per bit pass
+
 template <int C>
 struct __align__(16) WarpSmem {
-    uint32_t S[Cfg<C>::TW];
-    uint32_t alist[kACap];
-    uint32_t jptr[Cfg<C>::JPT + 1];
-    uint32_t boff[Cfg<C>::JPT + 1];
-    uint32_t mpa[kWarp];
-    uint32_t mpb[kWarp];
-    uint32_t mpre[kWarp + 1];
-    uint8_t mj[kWarp];
-    uint8_t bits[Cfg<C>::MAXBITS];
+    uint32_t S[Cfg<C>::TW];          // sample tile (dense path)
+    uint32_t alist[kACap];           // column blocks of row block I
+    uint32_t jptr[Cfg<C>::JPT + 1];  // indptr of the row blocks J_out of this tile
+    uint32_t upre[Cfg<C>::JPT + 1];  // search-unit prefix over active slices
+    uint32_t mc[Cfg<C>::JPT + 1];    // match-list start of each slice
+    uint32_t mpa[kMCap];             // matched tile of row block I
+    uint32_t mpb[kMCap];             // matched tile of row block J_out
+    uint16_t bits[kBCap];            // (row << 8) | column of the sample tile's set bits
 };
 
 __device__ __forceinline__ void mma_b1(int32_t (&c)[4], uint32_t a0, uint32_t a1, uint32_t b0)
@@ -80,6 +82,66 @@ __device__ __forceinline__ uint32_t slice_of(const uint32_t* S, int r, int j)
 {
     constexpr int WPR = Cfg<C>::WPR;
     return (S[r * WPR + ((16 * j) >> 5)] >> ((16 * j) & 31)) & 0xFFFFu;
+}
+
+// One bit pass: every set bit (r, col) of the sample tile, one per lane, adds
+// popc(L[I,K][r] & L[J_out,K][col % 16]) over the buffered matches K of its slice
+// j = col / 16, i.e. match-list entries [mc[j], mc[j+1]) clipped to [lo, hi).
+template <int C>
+__device__ __forceinline__ unsigned long long bit_pass(WarpSmem<C>& s, uint32_t w0, uint32_t w1,
+                                                       uint32_t e, uint32_t nnz, uint32_t lo,
+                                                       uint32_t hi,
+                                                       const uint32_t* __restrict__ blocks,
+                                                       int lane)
+{
+    constexpr int WPR = Cfg<C>::WPR, TW = Cfg<C>::TW;
+    unsigned long long acc = 0;
+    for (uint32_t bb = 0; bb < nnz; bb += kBCap) {
+        uint32_t idx = e;
+#pragma unroll
+        for (int q = 0; q < (C == 128 ? 2 : 1); ++q) {
+            uint32_t x = q == 0 ? w0 : w1;
+            while (x) {
+                const uint32_t b = __ffs(x) - 1;
+                x &= x - 1;
+                if (idx - bb < (uint32_t)kBCap) {
+                    uint32_t r, col;
+                    if constexpr (C == 128) {
+                        r = lane >> 1;
+                        col = 64u * (lane & 1) + 32u * q + b;
+                    } else {
+                        r = lane;
+                        col = b;
+                    }
+                    s.bits[idx - bb] = (uint16_t)((r << 8) | col);
+                }
+                ++idx;
+            }
+        }
+        __syncwarp();
+        const uint32_t nb = min((uint32_t)kBCap, nnz - bb);
+        for (uint32_t q = lane; q < nb; q += kWarp) {
+            const uint32_t code = s.bits[q];
+            const uint32_t r = code >> 8, col = code & 0xFFu;
+            const uint32_t j = col >> 4, c = col & 15u;
+            const uint32_t k0 = max(s.mc[j], lo), k1 = min(s.mc[j + 1], hi);
+            const uint32_t* Ar = blocks + r * WPR;
+            const uint32_t* Br = blocks + c * WPR;
+            for (uint32_t k = k0; k < k1; ++k) {
+                const size_t pa = s.mpa[k - lo], pb = s.mpb[k - lo];
+                if constexpr (C == 128) {
+                    const uint4 a = *reinterpret_cast<const uint4*>(Ar + pa * TW);
+                    const uint4 b = *reinterpret_cast<const uint4*>(Br + pb * TW);
+                    acc += (unsigned)(__popc(a.x & b.x) + __popc(a.y & b.y) + __popc(a.z & b.z) +
+                                      __popc(a.w & b.w));
+                } else {
+                    acc += (unsigned)__popc(Ar[pa * TW] & Br[pb * TW]);
+                }
+            }
+        }
+        __syncwarp();
+    }
+    return acc;
 }
 
 template <int C>
@@ -112,13 +174,8 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
             const uint2 v = reinterpret_cast<const uint2*>(blocks + (size_t)t * TW)[lane];
             w0 = v.x;
             w1 = v.y;
-            s.S[2 * lane] = w0;
-            s.S[2 * lane + 1] = w1;
         } else {
-            if (lane < 16) {
-                w0 = blocks[(size_t)t * TW + lane];
-                s.S[lane] = w0;
-            }
+            if (lane < 16) w0 = blocks[(size_t)t * TW + lane];
         }
         const int nnz = (int)__reduce_add_sync(kFull, (unsigned)(__popc(w0) + __popc(w1)));
 
@@ -165,94 +222,38 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
 
         if (nnz <= tau) {
             // ================= sparse path ===================================
-            // bit list grouped by slice, then row, then column
-            uint32_t excl[4] = {0, 0, 0, 0};
-            uint32_t tot[JPT];
-            if constexpr (C == 128) {
-                unsigned long long x = (unsigned long long)p[0] | ((unsigned long long)p[1] << 16) |
-                                       ((unsigned long long)p[2] << 32) |
-                                       ((unsigned long long)p[3] << 48);
-                const unsigned long long own = x;
+            // Search every element of the active slices' row-block lists in row block
+            // I's list (32 per round); matches are appended in slice order, so slice
+            // j owns match-list entries [mc[j], mc[j+1]).  Then one lane per set bit.
+            const uint32_t mine = (uint32_t)(__popc(w0) + __popc(w1));
+            uint32_t e = mine;  // exclusive count of set bits held by lower lanes
 #pragma unroll
-                for (int d = 2; d < 32; d <<= 1) {
-                    const unsigned long long y = __shfl_up_sync(kFull, x, d);
-                    if (lane >= d) x += y;
-                }
-                const unsigned long long e = x - own;
-                const unsigned long long t0 = __shfl_sync(kFull, x, 30);
-                const unsigned long long t1 = __shfl_sync(kFull, x, 31);
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    excl[q] = (uint32_t)(e >> (16 * q)) & 0xFFFFu;
-                    tot[q] = (uint32_t)(t0 >> (16 * q)) & 0xFFFFu;
-                    tot[4 + q] = (uint32_t)(t1 >> (16 * q)) & 0xFFFFu;
-                }
-            } else {
-                uint32_t x = (lane < 16) ? (p[0] | (p[1] << 16)) : 0u;
-                const uint32_t own = x;
-#pragma unroll
-                for (int d = 1; d < 16; d <<= 1) {
-                    const uint32_t y = __shfl_up_sync(kFull, x, d);
-                    if (lane >= d) x += y;
-                }
-                const uint32_t e = x - own;
-                const uint32_t t15 = __shfl_sync(kFull, x, 15);
-                excl[0] = e & 0xFFFFu;
-                excl[1] = e >> 16;
-                tot[0] = t15 & 0xFFFFu;
-                tot[1] = t15 >> 16;
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t y = __shfl_up_sync(kFull, e, d);
+                if (lane >= d) e += y;
             }
-            uint32_t boff[JPT + 1];
-            boff[0] = 0;
+            e -= mine;
+            if (lane == 0) {
 #pragma unroll
-            for (int j = 0; j < JPT; ++j) boff[j + 1] = boff[j] + tot[j];
-            if (lane <= JPT) {
-#pragma unroll
-                for (int j = 0; j <= JPT; ++j)
-                    if (lane == j) s.boff[j] = boff[j];
-            }
-            // write this lane's slices' bits
-            if constexpr (C == 128) {
-                const int r = lane >> 1, h = lane & 1;
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    uint32_t sl = ((q < 2 ? w0 : w1) >> (16 * (q & 1))) & 0xFFFFu;
-                    uint32_t pos = (h ? boff[4 + q] : boff[q]) + excl[q];
-                    while (sl) {
-                        const int c = __ffs(sl) - 1;
-                        sl &= sl - 1;
-                        s.bits[pos++] = (uint8_t)((r << 4) | c);
-                    }
-                }
-            } else if (lane < 16) {
-#pragma unroll
-                for (int q = 0; q < 2; ++q) {
-                    uint32_t sl = (w0 >> (16 * q)) & 0xFFFFu;
-                    uint32_t pos = boff[q] + excl[q];
-                    while (sl) {
-                        const int c = __ffs(sl) - 1;
-                        sl &= sl - 1;
-                        s.bits[pos++] = (uint8_t)((lane << 4) | c);
-                    }
-                }
+                for (int j = 0; j <= JPT; ++j) s.upre[j] = upre[j];
             }
             __syncwarp();
-
             const uint32_t W = upre[JPT];
+            uint32_t mc = 0;  // lane j <= JPT: matches so far from slices below j
+            uint32_t nm = 0, lo = 0;
             for (uint32_t ub = 0; ub < W; ub += kWarp) {
                 const uint32_t u = ub + lane;
                 bool found = false;
                 uint32_t pa = 0, pb = 0;
-                int jj = 0;
                 if (u < W) {
-                    uint32_t ustart = 0;
+                    uint32_t jb = s.jptr[0], us = 0;
 #pragma unroll
                     for (int j = 1; j < JPT; ++j)
                         if (u >= upre[j]) {
-                            jj = j;
-                            ustart = upre[j];
+                            jb = s.jptr[j];
+                            us = upre[j];
                         }
-                    pb = s.jptr[jj] + (u - ustart);
+                    pb = jb + (u - us);
                     const uint32_t b = indices[pb];
                     uint32_t pos;
                     if (stageA) {
@@ -265,56 +266,34 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
                     pa = startI + pos;
                 }
                 const unsigned mb = __ballot_sync(kFull, found);
-                if (mb == 0) continue;
-                const int nm = __popc(mb);
-                uint32_t cnt = 0;
                 if (found) {
-                    const int k = __popc(mb & lt);
+                    const uint32_t k = nm - lo + __popc(mb & lt);
                     s.mpa[k] = pa;
                     s.mpb[k] = pb;
-                    s.mj[k] = (uint8_t)jj;
                 }
-                __syncwarp();
-                if (lane < nm) {
-                    const int j = s.mj[lane];
-                    cnt = s.boff[j + 1] - s.boff[j];
+                if (lane <= JPT) {
+                    const uint32_t lim = s.upre[lane];
+                    const uint32_t below = lim <= ub ? 0u
+                                          : (lim - ub >= 32u ? kFull : ((1u << (lim - ub)) - 1u));
+                    mc += __popc(mb & below);
                 }
-                uint32_t incl = cnt;
-#pragma unroll
-                for (int d = 1; d < 32; d <<= 1) {
-                    const uint32_t y = __shfl_up_sync(kFull, incl, d);
-                    if (lane >= d) incl += y;
+                nm += __popc(mb);
+                if (nm - lo > (uint32_t)(kMCap - kWarp) || (ub + kWarp >= W && nm > lo)) {
+                    if (lane <= JPT) s.mc[lane] = mc;
+                    __syncwarp();
+                    acc += bit_pass<C>(s, w0, w1, e, (uint32_t)nnz, lo, nm, blocks, lane);
+                    lo = nm;
                 }
-                if (lane < nm) s.mpre[lane] = incl - cnt;
-                const uint32_t U = __shfl_sync(kFull, incl, 31);
-                if (lane == 0) s.mpre[nm] = U;
-                __syncwarp();
-                for (uint32_t v = lane; v < U; v += kWarp) {
-                    // match k: last k with mpre[k] <= v
-                    uint32_t lo = 0, hi = (uint32_t)nm;
-                    while (hi - lo > 1) {
-                        const uint32_t mid = (lo + hi) >> 1;
-                        if (s.mpre[mid] <= v) lo = mid;
-                        else hi = mid;
-                    }
-                    const int j = s.mj[lo];
-                    const uint32_t code = s.bits[s.boff[j] + (v - s.mpre[lo])];
-                    const uint32_t r = code >> 4, c = code & 15u;
-                    const uint32_t* A = blocks + (size_t)s.mpa[lo] * TW + r * WPR;
-                    const uint32_t* Bq = blocks + (size_t)s.mpb[lo] * TW + c * WPR;
-                    if constexpr (C == 128) {
-                        const uint4 a = *reinterpret_cast<const uint4*>(A);
-                        const uint4 b = *reinterpret_cast<const uint4*>(Bq);
-                        acc += (unsigned)(__popc(a.x & b.x) + __popc(a.y & b.y) +
-                                          __popc(a.z & b.z) + __popc(a.w & b.w));
-                    } else {
-                        acc += (unsigned)__popc(A[0] & Bq[0]);
-                    }
-                }
-                __syncwarp();
             }
         } else {
             // ================= dense path: binary tensor core ================
+            if constexpr (C == 128) {
+                s.S[2 * lane] = w0;
+                s.S[2 * lane + 1] = w1;
+            } else {
+                if (lane < 16) s.S[lane] = w0;
+            }
+            __syncwarp();
             for (int j = 0; j < JPT; ++j) {
                 if (!((active >> j) & 1u)) continue;
                 int32_t c0[4] = {0, 0, 0, 0}, c1[4] = {0, 0, 0, 0};

@@ -42,6 +42,8 @@ typedef struct CUstream_st* btc_stream_t;
 #define BTC_INPUT_ON_HOST 0x1u /* src/dst are host pointers (pinned or pageable) */
 #define BTC_ORIENT_DEGREE 0x2u /* relabel vertices by descending degree (ties by id)
                                   before orienting each edge to (max, min) */
+#define BTC_BUILD_RADIX 0x4u   /* number tiles with the radix-sort builder even when the
+                                  (row block, column block) cell bitmap would fit */
 
 /* Default dense/sparse switch: a tile takes the binary tensor-core path when its
  * popcount exceeds tau.  Pass BTC_TAU_DEFAULT to use the engine's value. */

@@ -40,12 +40,13 @@ def _cuda():
     torch.cuda.synchronize()
 
 
+@pytest.mark.parametrize("radix", [False, True], ids=["bitmap", "radix"])
 @pytest.mark.parametrize("tile_cols", [32, 128])
 @pytest.mark.parametrize("name", FIXTURES)
-def test_build_is_bitexact_and_count_matches(name, tile_cols):
+def test_build_is_bitexact_and_count_matches(name, tile_cols, radix):
     fx = load_golden()[name]
     src, dst, n = golden_graph(name)
-    g = BitBSR(_dev(src), _dev(dst), n, tile_cols)
+    g = BitBSR(_dev(src), _dev(dst), n, tile_cols, radix=radix)
     h = g.to_host()
     assert h["num_blocks"] == fx[f"tiles_{tile_cols}"]
     assert {k: _digest(h[k]) for k in ("indptr", "indices", "row_indices", "blocks")} == \
@@ -69,13 +70,14 @@ def test_tau_sweep_is_invariant(name, tile_cols):
         assert g.count(tau=tau) == fx["count"], tau
 
 
+@pytest.mark.parametrize("radix", [False, True], ids=["bitmap", "radix"])
 @pytest.mark.parametrize("name", ["rmat_12_16_s7", "rmat_15_16_s7_deg", "sbm_2000_8_s2",
                                   "stencil27_16", "K33"])
 @pytest.mark.parametrize("tile_cols", [32, 128])
-def test_degree_orientation(name, tile_cols):
+def test_degree_orientation(name, tile_cols, radix):
     fx = load_golden()[name]
     src, dst, n = golden_graph(name)
-    g = BitBSR(_dev(src), _dev(dst), n, tile_cols, orient_degree=True)
+    g = BitBSR(_dev(src), _dev(dst), n, tile_cols, orient_degree=True, radix=radix)
     assert g.num_tiles == fx[f"tiles_{tile_cols}_degree"]
     rp, col, _ = O.lower_csr(src, dst, n, "degree")
     ref = O.bitbsr_build(rp, col, n, tile_cols)
@@ -115,28 +117,30 @@ def test_duplicates_both_directions_and_selfloops():
     assert {k: _digest(v) for k, v in g.to_host().items() if k in fx["digest_128"]} == fx["digest_128"]
 
 
+@pytest.mark.parametrize("radix", [False, True], ids=["bitmap", "radix"])
 @pytest.mark.parametrize("tile_cols", [32, 128])
-def test_edge_cases(tile_cols):
+def test_edge_cases(tile_cols, radix):
+    B = lambda s, d, n, tc: BitBSR(s, d, n, tc, radix=radix)
     # empty graph
-    g = BitBSR(_dev(np.zeros(0)), _dev(np.zeros(0)), 100, tile_cols)
+    g = B(_dev(np.zeros(0)), _dev(np.zeros(0)), 100, tile_cols)
     assert g.num_tiles == 0 and g.count() == 0
     h = g.to_host()
     assert np.all(h["indptr"] == 0) and len(h["indptr"]) == (100 + 15) // 16 + 1
     # only self-loops
     v = np.arange(50, dtype=np.int32)
-    g = BitBSR(_dev(v), _dev(v), 50, tile_cols)
+    g = B(_dev(v), _dev(v), 50, tile_cols)
     assert g.num_tiles == 0 and g.count() == 0
     # zero vertices
-    g = BitBSR(_dev(np.zeros(0)), _dev(np.zeros(0)), 0, tile_cols)
+    g = B(_dev(np.zeros(0)), _dev(np.zeros(0)), 0, tile_cols)
     assert g.count() == 0
     # one triangle at the last ids of a ragged n
     n = 1000
-    g = BitBSR(_dev([999, 998, 999]), _dev([998, 997, 997]), n, tile_cols)
+    g = B(_dev([999, 998, 999]), _dev([998, 997, 997]), n, tile_cols)
     assert g.count() == 1 and g.num_edges == 3
     # one full 16 x C tile (all-ones under the diagonal) and K_n closed forms
     for k in (16, 17, 31, 32, 33, 129, 200):
         s, d, _ = G.complete(k)
-        assert BitBSR(_dev(s), _dev(d), k, tile_cols).count() == comb(k, 3)
+        assert B(_dev(s), _dev(d), k, tile_cols).count() == comb(k, 3)
 
 
 def test_out_of_range_ids_are_rejected():
@@ -270,7 +274,7 @@ def test_rmat_scale18_orders_and_paths_agree():
     counts = set()
     for C in (32, 128):
         for deg in (False, True):
-            g = BitBSR(_dev(src), _dev(dst), n, C, orient_degree=deg)
+            g = BitBSR(_dev(src), _dev(dst), n, C, orient_degree=deg, radix=deg and C == 32)
             counts.add(g.count())
             counts.add(g.count(tau=0))
             counts.add(g.count(tau=_lib.BTC_TAU_ALL_SPARSE))
