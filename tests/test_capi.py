@@ -96,3 +96,29 @@ def test_header_compiles_as_c_and_cpp(tmp_path):
                     "-o", str(tmp_path / "t.o")], check=True)
     subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-I", inc, "-c", str(src),
                     "-o", str(tmp_path / "t2.o")], check=True)
+
+
+def test_compat_app_is_built_and_prints_usage():
+    """apps/btc_tc_lite.cu (the reference's BTC-Lite CLI over include/btc_compat.hpp)."""
+    app = os.path.join(os.path.dirname(_lib.LIB_PATH), "btc_tc_lite")
+    assert os.path.exists(app)
+    out = subprocess.run([app], capture_output=True, text=True)
+    assert out.returncode == 1 and "Usage" in out.stdout
+
+
+def test_compat_header_compiles_with_nvcc(tmp_path):
+    """include/btc_compat.hpp gives the reference's namespace-btc names and signatures."""
+    src = tmp_path / "c.cu"
+    src.write_text(
+        '#include "btc_compat.hpp"\n'
+        "struct Coo { int num_rows; size_t num_entries;\n"
+        "  thrust::device_vector<int> row_indices, column_indices; };\n"
+        "unsigned long long f(Coo& coo) {\n"
+        "  btc::BCSR_16x128_Device a; btc::convert_coo_to_bcsr_16x128_gpu(a, coo);\n"
+        "  float ms; unsigned long long c = btc::count_triangles_16x128_adaptive(a, 2048, &ms);\n"
+        "  btc::BCSR_16x32_Device b; btc::convert_coo_to_bcsr_16x32_gpu(b, coo);\n"
+        "  c += btc::count_triangles_16x32_adaptive(b); c += a.get_result(); a.reset_result();\n"
+        "  a.free(); b.free(); return c; }\n")
+    subprocess.run(["nvcc", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-I",
+                    os.path.join(ROOT, "include"), "-c", str(src), "-o", str(tmp_path / "c.o")],
+                   check=True)

@@ -280,3 +280,24 @@ def test_rmat_scale18_orders_and_paths_agree():
             counts.add(g.count(tau=_lib.BTC_TAU_ALL_SPARSE))
             g.free()
     assert counts == {want}
+
+
+@pytest.mark.parametrize("name", ["stencil27_16", "rmat_12_16_s7", "K130"])
+def test_compat_cli_reads_reference_bin_format(name, tmp_path):
+    """apps/btc_tc_lite.cu: the reference's CLI flow over btc_compat.hpp, fed the
+    reference's binary CSR file, prints the reference's result line."""
+    import os
+    import re
+    import subprocess
+    fx = load_golden()[name]
+    src, dst, n = golden_graph(name)
+    rp, col, _ = O.lower_csr(src, dst, n)
+    path = tmp_path / f"{name}.bin"
+    G.write_bin_csr(str(path), rp, col, n)
+    app = os.path.join(os.path.dirname(_lib.LIB_PATH), "btc_tc_lite")
+    for mode in ("0", "1", "2"):
+        out = subprocess.run([app, "-i", str(path), "-w", "1", "-r", "3"], capture_output=True,
+                             text=True, env={**os.environ, "BTC_MODE": mode}, timeout=120)
+        assert out.returncode == 0, out.stdout + out.stderr
+        got = int(re.search(r"Triangles \(GPU\): (\d+)", out.stdout).group(1))
+        assert got == fx["count"], (mode, out.stdout)
