@@ -44,6 +44,7 @@ EXPORTS = [
     "btc_default_tau",
     "btc_strerror",
     "btc_abi_version",
+    "btc_count_bcsr_noalloc",
 ]
 
 
@@ -117,6 +118,7 @@ def lib():
         L.btc_strerror.argtypes = [C.c_int]
         L.btc_strerror.restype = C.c_char_p
         L.btc_abi_version.argtypes = []
+        L.btc_count_bcsr_noalloc.argtypes = [P(BtcBcsrDevice), C.c_int, C.c_int, vp, vp]
         for name in EXPORTS:
             if name not in ("btc_bcsr_free", "btc_free", "btc_strerror"):
                 getattr(L, name).restype = C.c_int

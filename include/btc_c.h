@@ -157,6 +157,24 @@ BTC_API int btc_rebuild_bitbsr(btc_bitbsr* g, const int32_t* src, const int32_t*
 BTC_API int btc_count(btc_bitbsr* g, int tau, btc_stream_t stream, unsigned long long* out_count,
               float* kernel_ms);
 
+/* Counts the triangles of a Bit-BSR without allocating any memory.  No counterpart in
+ * the reference: it exists for callers that cannot let a library call cudaMalloc, such
+ * as a serving process whose memory pool already holds the device's free memory, or a
+ * latency-bound loop that must not call cudaMalloc/cudaFree because they can synchronise
+ * the device.  The caller passes the Bit-BSR (reference layout, e.g. from
+ * btc_bitbsr_info or btc_convert_*) and a device word d_out for the count (NULL: use
+ * bcsr->result).  The count kernel's scratch (one partial sum per CTA plus a completion
+ * counter) is a fixed array inside the library's device image: 2048 partial-sum slots,
+ * 16,392 bytes, held by every GPU that loads the library until the process exits.  A GPU
+ * whose count grid needs more than 2048 CTAs is rejected with BTC_E_INVAL and a message
+ * on stderr (a B200 needs 592).  The first call on each device looks up the array's
+ * device address (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture.  All calls share the one array: calls whose kernels overlap
+ * on the GPU (different streams, or several host threads) race and give wrong counts, so
+ * order them.  Stream-ordered; does not wait for the result.  tau as in btc_count. */
+BTC_API int btc_count_bcsr_noalloc(const btc_bcsr_device* bcsr, int tile_cols, int tau,
+                                   btc_stream_t stream, unsigned long long* d_out);
+
 /* Enqueues the count on `stream` without waiting; the uint64 count lands in device
  * memory at d_out (nullable: then only in the handle's result slot) when the
  * stream reaches it. */
