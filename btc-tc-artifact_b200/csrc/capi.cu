@@ -113,8 +113,8 @@ static int ensure_count_scratch(btc_bitbsr* g)
     const size_t need = sizeof(unsigned long long) * (size_t)grid;
     if (g->partials.bytes < need) BTC_TRY(g->partials.reserve(need));
     if (!g->done.ptr) {
-        BTC_TRY(g->done.reserve(sizeof(unsigned int)));
-        BTC_CUDA_TRY(cudaMemset(g->done.ptr, 0, sizeof(unsigned int)));
+        BTC_TRY(g->done.reserve(kCountCtlBytes));
+        BTC_CUDA_TRY(cudaMemset(g->done.ptr, 0, kCountCtlBytes));
     }
     if (!g->result.ptr) {
         BTC_TRY(g->result.reserve(sizeof(unsigned long long)));
@@ -267,10 +267,12 @@ static int count_handle(btc_bitbsr* g, int tau, cudaStream_t s, unsigned long lo
     if (tau < 0) return BTC_E_INVAL;
     BTC_TRY(ensure_count_scratch(g));
     CountScratch scr{g->partials.as<unsigned long long>(), g->done.as<unsigned int>(),
+                     reinterpret_cast<unsigned long long*>(g->done.as<char>() + 8),
                      g->result.as<unsigned long long>(), d_out2};
+    const int64_t ncb = ((int64_t)g->n + g->tile_cols - 1) / g->tile_cols;
     return launch_count(g->tile_cols, g->indptr.as<uint32_t>(), g->indices.as<uint32_t>(),
                         g->row_indices.as<uint32_t>(), g->blocks.as<uint32_t>(), g->num_tiles,
-                        g->n_row_blocks, tau, scr, s);
+                        g->n_row_blocks, ncb, tau, scr, s);
 }
 
 // ===========================================================================
@@ -509,8 +511,8 @@ static int count_struct(btc_bcsr_device* b, int tile_cols, float* kernel_ms,
     const size_t need = sizeof(unsigned long long) * (size_t)count_grid_size(tile_cols);
     if (ss.partials[dev].bytes < need) BTC_TRY(ss.partials[dev].reserve(need));
     if (!ss.done[dev].ptr) {
-        BTC_TRY(ss.done[dev].reserve(sizeof(unsigned int)));
-        BTC_CUDA_TRY(cudaMemset(ss.done[dev].ptr, 0, sizeof(unsigned int)));
+        BTC_TRY(ss.done[dev].reserve(kCountCtlBytes));
+        BTC_CUDA_TRY(cudaMemset(ss.done[dev].ptr, 0, kCountCtlBytes));
     }
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (kernel_ms) {
@@ -519,9 +521,11 @@ static int count_struct(btc_bcsr_device* b, int tile_cols, float* kernel_ms,
         BTC_CUDA_TRY(cudaEventRecord(e0, nullptr));
     }
     CountScratch scr{ss.partials[dev].as<unsigned long long>(), ss.done[dev].as<unsigned int>(),
-                     b->result, nullptr};
+                     reinterpret_cast<unsigned long long*>(ss.done[dev].as<char>() + 8), b->result,
+                     nullptr};
+    const int64_t ncb = ((int64_t)b->n + tile_cols - 1) / tile_cols;
     int st = launch_count(tile_cols, b->indptr, b->indices, b->row_indices, b->blocks, b->num_blocks,
-                          b->n_row_blocks, default_tau(tile_cols), scr, nullptr);
+                          b->n_row_blocks, ncb, default_tau(tile_cols), scr, nullptr);
     if (st == BTC_OK && kernel_ms && cudaEventRecord(e1, nullptr) != cudaSuccess) st = BTC_E_CUDA;
     if (st == BTC_OK && cudaMemcpy(out, b->result, sizeof(unsigned long long),
                                    cudaMemcpyDeviceToHost) != cudaSuccess)

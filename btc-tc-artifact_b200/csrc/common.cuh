@@ -137,6 +137,7 @@ BuildGeom make_geom(int32_t n, int tile_cols);
 struct CountScratch {
     unsigned long long* partials;  // one per CTA of the persistent grid
     unsigned int* done;            // CTAs finished (reset to 0 by the last one)
+    unsigned long long* work;      // tile queue head (reset to 0 by the last CTA)
     unsigned long long* result;    // where the final count lands
     unsigned long long* result2;   // optional second destination (nullable)
 };
@@ -144,7 +145,11 @@ struct CountScratch {
 int count_grid_size(int tile_cols);
 int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
                  const uint32_t* row_indices, const uint32_t* blocks, uint32_t num_tiles,
-                 int32_t n_row_blocks, int tau, CountScratch scr, cudaStream_t s);
+                 int32_t n_row_blocks, int64_t n_col_blocks, int tau, CountScratch scr,
+                 cudaStream_t s);
+
+// Queue/completion words of the count kernel: done (u32) at byte 0, work (u64) at 8.
+constexpr size_t kCountCtlBytes = 16;
 
 int device_sm_count();
 

@@ -8,17 +8,23 @@
 // Integer arithmetic only; per-lane uint64 partials, one uint64 per CTA, and the last
 // CTA to finish adds the per-CTA partials (no floating point, no spin-waits).
 //
-// Work mapping (one warp per sample tile, persistent grid-stride over tiles):
+// Work mapping (persistent grid; each warp takes runs of consecutive tiles from a
+// global queue, so the tiles of one row block usually stay with one warp):
+//  * Row block I's column-block list is staged once per row block, as a shared-memory
+//    bitmap with per-word prefix counts (membership and rank in O(1)) when the graph has
+//    at most 8192 column blocks, else as a sorted list (binary search).
 //  * S is loaded once (one 8-byte load per lane for 16x128); its popcount picks the
 //    path: > tau -> binary tensor core, else CUDA cores.
 //  * The row blocks J_out = J_L*(C/16) + j are consecutive, so their index lists form
-//    one contiguous run of indices[]; the warp searches every element of the lists of
-//    the slices that have bits (32 at a time, one per lane) in row block I's list,
-//    which is staged in shared memory when short.  This replaces the reference's
-//    serial two-pointer merge, repeated per slice by all 32 lanes, with one parallel
-//    search per tile.
-//  * Sparse path: matches of a round are compacted; (match, mask bit) units are spread
-//    over the lanes; each unit is one 16-byte AND + 4 popc (16x128) or one word (16x32).
+//    one contiguous run of indices[]; the warp looks up every element of the lists of
+//    the slices that have bits (32 per round, one per lane) in row block I's structure.
+//    This replaces the reference's serial two-pointer merge, repeated per slice by all
+//    32 lanes, with one parallel search per tile.
+//  * Sparse path: matches are appended in slice order (slice j owns entries
+//    [mc[j], mc[j+1])).  Each set bit (r, c) of S then adds popc(L[I,K][r] & L[J_out,K][c])
+//    over its slice's matches, with the lanes spread over bits (many bits, few matches:
+//    stencils) or over the matches of one bit at a time (few bits, many matches:
+//    Erdos-Renyi, R-MAT).  One unit is one 16-byte AND + 4 popc (16x128) or one word.
 //  * Dense path: per slice, every match feeds mma.sync.m16n8k128.row.col.s32.b1.b1.s32
 //    .and.popc twice (16x16 popcount block), masked by the slice's bits.  16x32 tiles
 //    pack four matches into the 128-bit k dimension, as tc_16x32_mma_v6.h:72-154 does.
@@ -30,7 +36,10 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / kWarp;
-constexpr int kACap = 256;  // row-block list entries staged in shared memory per warp
+constexpr int kACap = 256;     // list mode: row-block list entries staged per warp
+constexpr int kBmWords = 256;  // bitmap mode: graphs with at most 8192 column blocks
+constexpr int kMCap = 64;      // matches buffered per warp before a bit pass
+constexpr int kBCap = 512;     // mask-bit codes buffered per warp per bit pass
 
 template <int C>
 struct Cfg {
@@ -40,19 +49,28 @@ struct Cfg {
     static constexpr int MAXBITS = 16 * C;   // bits per tile
 };
 
-constexpr int kMCap = 64;   // matches buffered per warp before a bit pass
-constexpr int kBCap = 512;  // mask-bit codes buffered per warp per bit pass
-
 template <int C>
 struct __align__(16) WarpSmem {
     uint32_t S[Cfg<C>::TW];          // sample tile (dense path)
-    uint32_t alist[kACap];           // column blocks of row block I
+    union {
+        uint32_t list[kACap];        // row block I's column blocks (list mode)
+        uint32_t bm[kBmWords];       // the same as a bitmap (bitmap mode)
+    } a;
+    uint16_t apre[kBmWords];         // bitmap mode: list entries below each word
     uint32_t jptr[Cfg<C>::JPT + 1];  // indptr of the row blocks J_out of this tile
     uint32_t upre[Cfg<C>::JPT + 1];  // search-unit prefix over active slices
     uint32_t mc[Cfg<C>::JPT + 1];    // match-list start of each slice
     uint32_t mpa[kMCap];             // matched tile of row block I
     uint32_t mpb[kMCap];             // matched tile of row block J_out
     uint16_t bits[kBCap];            // (row << 8) | column of the sample tile's set bits
+};
+
+// Row block I's column-block list as the search structure of the current tile.
+struct ARow {
+    uint32_t start;  // indptr[I]
+    uint32_t len;    // number of tiles in row block I
+    uint32_t words;  // bitmap mode: bitmap words in use
+    int mode;        // 0: sorted list in shared memory, 1: bitmap, 2: sorted list in HBM
 };
 
 __device__ __forceinline__ void mma_b1(int32_t (&c)[4], uint32_t a0, uint32_t a1, uint32_t b0)
@@ -82,6 +100,83 @@ __device__ __forceinline__ uint32_t slice_of(const uint32_t* S, int r, int j)
 {
     constexpr int WPR = Cfg<C>::WPR;
     return (S[r * WPR + ((16 * j) >> 5)] >> ((16 * j) & 31)) & 0xFFFFu;
+}
+
+// Stages row block I's column-block list for lookups.  Called with the warp converged.
+template <int C>
+__device__ __forceinline__ ARow stage_row(WarpSmem<C>& s, const uint32_t* __restrict__ indptr,
+                                          const uint32_t* __restrict__ indices, uint32_t I,
+                                          bool bitmap_ok, int lane)
+{
+    ARow A;
+    A.start = indptr[I];
+    A.len = indptr[I + 1] - A.start;  // >= 1: a tile of row block I is being counted
+    A.words = 0;
+    __syncwarp();  // earlier readers of s.a / s.apre are done
+    if (bitmap_ok) {
+        A.mode = 1;
+        A.words = (indices[A.start + A.len - 1] >> 5) + 1;  // <= kBmWords
+        for (uint32_t w = lane; w < A.words; w += kWarp) s.a.bm[w] = 0u;
+        __syncwarp();
+        for (uint32_t i = lane; i < A.len; i += kWarp) {
+            const uint32_t k = indices[A.start + i];
+            atomicOr(&s.a.bm[k >> 5], 1u << (k & 31u));
+        }
+        __syncwarp();
+        // per-word exclusive prefix; lane owns words [8*lane, 8*lane + 8)
+        uint32_t cnt[8], tot = 0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const uint32_t w = 8u * lane + q;
+            cnt[q] = w < A.words ? __popc(s.a.bm[w]) : 0u;
+            tot += cnt[q];
+        }
+        uint32_t incl = tot;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(kFull, incl, d);
+            if (lane >= d) incl += y;
+        }
+        uint32_t run = incl - tot;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const uint32_t w = 8u * lane + q;
+            if (w < A.words) s.apre[w] = (uint16_t)run;
+            run += cnt[q];
+        }
+    } else if (A.len <= (uint32_t)kACap) {
+        A.mode = 0;
+        for (uint32_t i = lane; i < A.len; i += kWarp) s.a.list[i] = indices[A.start + i];
+    } else {
+        A.mode = 2;
+    }
+    __syncwarp();
+    return A;
+}
+
+// Is column block b in row block I?  If so, pa = its tile index.
+template <int C>
+__device__ __forceinline__ bool a_lookup(const WarpSmem<C>& s, const ARow& A,
+                                         const uint32_t* __restrict__ indices, uint32_t b,
+                                         uint32_t& pa)
+{
+    if (A.mode == 1) {
+        const uint32_t w = b >> 5;
+        if (w >= A.words) return false;
+        const uint32_t x = s.a.bm[w];
+        const uint32_t bit = 1u << (b & 31u);
+        if (!(x & bit)) return false;
+        pa = A.start + s.apre[w] + __popc(x & (bit - 1u));
+        return true;
+    }
+    if (A.mode == 0) {
+        const uint32_t pos = lower_bound_u32(s.a.list, A.len, b);
+        pa = A.start + pos;
+        return pos < A.len && s.a.list[pos] == b;
+    }
+    const uint32_t pos = lower_bound_u32(indices + A.start, A.len, b);
+    pa = A.start + pos;
+    return pos < A.len && indices[A.start + pos] == b;
 }
 
 // One bit pass: every set bit (r, col) of the sample tile, one per lane, adds
@@ -120,22 +215,46 @@ __device__ __forceinline__ unsigned long long bit_pass(WarpSmem<C>& s, uint32_t 
         }
         __syncwarp();
         const uint32_t nb = min((uint32_t)kBCap, nnz - bb);
-        for (uint32_t q = lane; q < nb; q += kWarp) {
-            const uint32_t code = s.bits[q];
-            const uint32_t r = code >> 8, col = code & 0xFFu;
-            const uint32_t j = col >> 4, c = col & 15u;
-            const uint32_t k0 = max(s.mc[j], lo), k1 = min(s.mc[j + 1], hi);
-            const uint32_t* Ar = blocks + r * WPR;
-            const uint32_t* Br = blocks + c * WPR;
-            for (uint32_t k = k0; k < k1; ++k) {
-                const size_t pa = s.mpa[k - lo], pb = s.mpb[k - lo];
-                if constexpr (C == 128) {
-                    const uint4 a = *reinterpret_cast<const uint4*>(Ar + pa * TW);
-                    const uint4 b = *reinterpret_cast<const uint4*>(Br + pb * TW);
-                    acc += (unsigned)(__popc(a.x & b.x) + __popc(a.y & b.y) + __popc(a.z & b.z) +
-                                      __popc(a.w & b.w));
-                } else {
-                    acc += (unsigned)__popc(Ar[pa * TW] & Br[pb * TW]);
+        if (2 * nb <= hi - lo || nb <= 2) {
+            // few bits, many matches: one bit at a time, lanes over its slice's matches
+            for (uint32_t q = 0; q < nb; ++q) {
+                const uint32_t code = s.bits[q];
+                const uint32_t r = code >> 8, col = code & 0xFFu;
+                const uint32_t j = col >> 4, c = col & 15u;
+                const uint32_t k0 = max(s.mc[j], lo), k1 = min(s.mc[j + 1], hi);
+                const uint32_t* Ar = blocks + r * WPR;
+                const uint32_t* Br = blocks + c * WPR;
+                for (uint32_t k = k0 + lane; k < k1; k += kWarp) {
+                    const size_t pa = s.mpa[k - lo], pb = s.mpb[k - lo];
+                    if constexpr (C == 128) {
+                        const uint4 a = *reinterpret_cast<const uint4*>(Ar + pa * TW);
+                        const uint4 b = *reinterpret_cast<const uint4*>(Br + pb * TW);
+                        acc += (unsigned)(__popc(a.x & b.x) + __popc(a.y & b.y) +
+                                          __popc(a.z & b.z) + __popc(a.w & b.w));
+                    } else {
+                        acc += (unsigned)__popc(Ar[pa * TW] & Br[pb * TW]);
+                    }
+                }
+            }
+        } else {
+            // many bits: lanes over bits, each walking its slice's matches
+            for (uint32_t q = lane; q < nb; q += kWarp) {
+                const uint32_t code = s.bits[q];
+                const uint32_t r = code >> 8, col = code & 0xFFu;
+                const uint32_t j = col >> 4, c = col & 15u;
+                const uint32_t k0 = max(s.mc[j], lo), k1 = min(s.mc[j + 1], hi);
+                const uint32_t* Ar = blocks + r * WPR;
+                const uint32_t* Br = blocks + c * WPR;
+                for (uint32_t k = k0; k < k1; ++k) {
+                    const size_t pa = s.mpa[k - lo], pb = s.mpb[k - lo];
+                    if constexpr (C == 128) {
+                        const uint4 a = *reinterpret_cast<const uint4*>(Ar + pa * TW);
+                        const uint4 b = *reinterpret_cast<const uint4*>(Br + pb * TW);
+                        acc += (unsigned)(__popc(a.x & b.x) + __popc(a.y & b.y) +
+                                          __popc(a.z & b.z) + __popc(a.w & b.w));
+                    } else {
+                        acc += (unsigned)__popc(Ar[pa * TW] & Br[pb * TW]);
+                    }
                 }
             }
         }
@@ -145,10 +264,11 @@ __device__ __forceinline__ unsigned long long bit_pass(WarpSmem<C>& s, uint32_t 
 }
 
 template <int C>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 4)
 k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
         const uint32_t* __restrict__ row_indices, const uint32_t* __restrict__ blocks,
-        uint32_t num_tiles, int32_t R, int tau, CountScratch scr)
+        uint32_t num_tiles, int32_t R, int64_t n_col_blocks, int tau, uint32_t chunk,
+        CountScratch scr)
 {
     using K = Cfg<C>;
     constexpr int WPR = K::WPR, TW = K::TW, JPT = K::JPT;
@@ -162,55 +282,67 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
     const int g = lane >> 2, tg = lane & 3;  // mma fragment coordinates
 
     unsigned long long acc = 0;
+    const bool bitmap_ok = n_col_blocks <= (int64_t)kBmWords * 32;
 
-    for (uint64_t t = (uint64_t)blockIdx.x * kWarps + warp; t < num_tiles;
-         t += (uint64_t)gridDim.x * kWarps) {
-        const uint32_t I = row_indices[t];
-        const uint32_t JL = indices[t];
+    for (;;) {
+      unsigned long long c0 = 0;
+      if (lane == 0) c0 = atomicAdd(scr.work, (unsigned long long)chunk);
+      c0 = __shfl_sync(kFull, c0, 0);
+      if (c0 >= num_tiles) break;
+      const uint32_t c1 = (uint32_t)min(c0 + chunk, (unsigned long long)num_tiles);
+      uint32_t curI = 0xffffffffu;
+      ARow A{0, 0, 0, 0};
+      // the next tile's ids and sample words are loaded one tile ahead
+      uint32_t nI = row_indices[c0], nJL = indices[c0], nw0 = 0, nw1 = 0;
+      if constexpr (C == 128) {
+          const uint2 v = reinterpret_cast<const uint2*>(blocks + (size_t)c0 * TW)[lane];
+          nw0 = v.x;
+          nw1 = v.y;
+      } else {
+          if (lane < 16) nw0 = blocks[(size_t)c0 * TW + lane];
+      }
+      for (uint32_t t = (uint32_t)c0; t < c1; ++t) {
+        const uint32_t I = nI, JL = nJL, w0 = nw0, w1 = nw1;
+        if (t + 1 < c1) {
+            nI = row_indices[t + 1];
+            nJL = indices[t + 1];
+            if constexpr (C == 128) {
+                const uint2 v = reinterpret_cast<const uint2*>(blocks + (size_t)(t + 1) * TW)[lane];
+                nw0 = v.x;
+                nw1 = v.y;
+            } else {
+                if (lane < 16) nw0 = blocks[(size_t)(t + 1) * TW + lane];
+            }
+        }
 
         // ---- sample tile and its slices -------------------------------------
-        uint32_t w0 = 0, w1 = 0;
-        if constexpr (C == 128) {
-            const uint2 v = reinterpret_cast<const uint2*>(blocks + (size_t)t * TW)[lane];
-            w0 = v.x;
-            w1 = v.y;
-        } else {
-            if (lane < 16) w0 = blocks[(size_t)t * TW + lane];
-        }
         const int nnz = (int)__reduce_add_sync(kFull, (unsigned)(__popc(w0) + __popc(w1)));
 
-        // per-lane slice popcounts, packed 16 bits per slice
         // 16x128: lane = 2r + h holds slices j = 4h + q (q = 0..3) of row r
         // 16x32 : lane = r (< 16) holds slices j = q (q = 0..1) of row r
-        uint32_t p[4];
-        p[0] = __popc(w0 & 0xFFFFu);
-        p[1] = __popc(w0 >> 16);
-        p[2] = __popc(w1 & 0xFFFFu);
-        p[3] = __popc(w1 >> 16);
-
         uint32_t active = 0;  // bit j set if slice j has any bit
         if constexpr (C == 128) {
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                const unsigned b = __ballot_sync(kFull, p[q] != 0);
+                const uint32_t sl = ((q < 2 ? w0 : w1) >> (16 * (q & 1))) & 0xFFFFu;
+                const unsigned b = __ballot_sync(kFull, sl != 0);
                 if (b & 0x55555555u) active |= 1u << q;
                 if (b & 0xAAAAAAAAu) active |= 1u << (4 + q);
             }
         } else {
 #pragma unroll
             for (int q = 0; q < 2; ++q)
-                if (__ballot_sync(kFull, p[q] != 0)) active |= 1u << q;
+                if (__ballot_sync(kFull, ((w0 >> (16 * q)) & 0xFFFFu) != 0)) active |= 1u << q;
         }
 
-        const uint32_t startI = indptr[I];
-        const uint32_t LA = indptr[I + 1] - startI;
+        if (I != curI) {
+            A = stage_row<C>(s, indptr, indices, I, bitmap_ok, lane);
+            curI = I;
+        }
         if (lane <= JPT) {
             const int64_t J = (int64_t)JL * JPT + lane;
             s.jptr[lane] = indptr[J < R ? J : R];
         }
-        const bool stageA = LA <= (uint32_t)kACap;
-        if (stageA)
-            for (uint32_t i = lane; i < LA; i += kWarp) s.alist[i] = indices[startI + i];
         __syncwarp();
 
         // unit prefix over active slices
@@ -254,16 +386,7 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
                             us = upre[j];
                         }
                     pb = jb + (u - us);
-                    const uint32_t b = indices[pb];
-                    uint32_t pos;
-                    if (stageA) {
-                        pos = lower_bound_u32(s.alist, LA, b);
-                        found = pos < LA && s.alist[pos] == b;
-                    } else {
-                        pos = lower_bound_u32(indices + startI, LA, b);
-                        found = pos < LA && indices[startI + pos] == b;
-                    }
-                    pa = startI + pos;
+                    found = a_lookup<C>(s, A, indices, indices[pb], pa);
                 }
                 const unsigned mb = __ballot_sync(kFull, found);
                 if (found) {
@@ -304,16 +427,7 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
                     uint32_t pa = 0, pb = 0;
                     if (u < je) {
                         pb = u;
-                        const uint32_t b = indices[pb];
-                        uint32_t pos;
-                        if (stageA) {
-                            pos = lower_bound_u32(s.alist, LA, b);
-                            found = pos < LA && s.alist[pos] == b;
-                        } else {
-                            pos = lower_bound_u32(indices + startI, LA, b);
-                            found = pos < LA && indices[startI + pos] == b;
-                        }
-                        pa = startI + pos;
+                        found = a_lookup<C>(s, A, indices, indices[pb], pa);
                     }
                     const unsigned mb = __ballot_sync(kFull, found);
                     if (mb == 0) continue;
@@ -367,6 +481,7 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
             }
         }
         __syncwarp();
+      }
     }
 
     // ---- int64 block tree + last-CTA reduction ------------------------------
@@ -397,6 +512,7 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
             *scr.result = total;
             if (scr.result2) *scr.result2 = total;
             *scr.done = 0u;
+            *scr.work = 0ull;
         }
     }
 }
@@ -417,15 +533,23 @@ int count_grid_size(int tile_cols)
 
 int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
                  const uint32_t* row_indices, const uint32_t* blocks, uint32_t num_tiles,
-                 int32_t n_row_blocks, int tau, CountScratch scr, cudaStream_t s)
+                 int32_t n_row_blocks, int64_t n_col_blocks, int tau, CountScratch scr,
+                 cudaStream_t s)
 {
     const int grid = count_grid_size(tile_cols);
+    // About eight queue grabs per warp, between 8 and 64 consecutive tiles per grab: the
+    // queue head is one word, and every grab is an atomic on it.
+    const uint64_t warps = (uint64_t)grid * kWarps;
+    uint64_t chunk = num_tiles / (warps * 8);
+    if (chunk < 8) chunk = 8;
+    if (chunk > 64) chunk = 64;
     if (tile_cols == 128)
         k_count<128><<<grid, kThreads, 0, s>>>(indptr, indices, row_indices, blocks, num_tiles,
-                                               n_row_blocks, tau, scr);
+                                               n_row_blocks, n_col_blocks, tau, (uint32_t)chunk,
+                                               scr);
     else
         k_count<32><<<grid, kThreads, 0, s>>>(indptr, indices, row_indices, blocks, num_tiles,
-                                              n_row_blocks, tau, scr);
+                                              n_row_blocks, n_col_blocks, tau, (uint32_t)chunk, scr);
     return cudaGetLastError() == cudaSuccess ? BTC_OK : BTC_E_CUDA;
 }
 

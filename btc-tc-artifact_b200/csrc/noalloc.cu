@@ -19,10 +19,11 @@ namespace btc200 {
 namespace {
 
 // Slots [0, kNoAllocMaxCtas) hold one partial sum per CTA of the count kernel; slot
-// kNoAllocMaxCtas holds the CTA completion counter.  (2048 + 1) x 8 bytes = 16,392
-// bytes, present on every GPU that loads the library until the process exits.
+// kNoAllocMaxCtas holds the CTA completion counter and the next slot the tile-queue
+// head.  (2048 + 2) x 8 bytes = 16,400 bytes, present on every GPU that loads the
+// library until the process exits.
 constexpr int kNoAllocMaxCtas = 2048;
-static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocMaxCtas + 1];
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocMaxCtas + 2];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mu;
@@ -76,11 +77,13 @@ extern "C" int btc_count_bcsr_noalloc(const btc_bcsr_device* b, int tile_cols, i
     unsigned long long* scratch = nullptr;
     BTC_TRY(scratch_for_current_device(&scratch));
 
-    // The completion counter must start at zero.  The kernel's last CTA puts it back to
-    // zero, so this only matters after an interrupted launch, but it costs nothing.
-    BTC_CUDA_TRY(cudaMemsetAsync(scratch + kNoAllocMaxCtas, 0, sizeof(unsigned long long), stream));
-    CountScratch scr{scratch, reinterpret_cast<unsigned int*>(scratch + kNoAllocMaxCtas), out,
-                     nullptr};
+    // The completion counter and the queue head must start at zero.  The kernel's last
+    // CTA puts both back to zero, so this only matters after an interrupted launch.
+    BTC_CUDA_TRY(
+        cudaMemsetAsync(scratch + kNoAllocMaxCtas, 0, 2 * sizeof(unsigned long long), stream));
+    CountScratch scr{scratch, reinterpret_cast<unsigned int*>(scratch + kNoAllocMaxCtas),
+                     scratch + kNoAllocMaxCtas + 1, out, nullptr};
+    const int64_t ncb = ((int64_t)b->n + tile_cols - 1) / tile_cols;
     return launch_count(tile_cols, b->indptr, b->indices, b->row_indices, b->blocks, b->num_blocks,
-                        b->n_row_blocks, tau, scr, stream);
+                        b->n_row_blocks, ncb, tau, scr, stream);
 }

@@ -164,8 +164,8 @@ BTC_API int btc_count(btc_bitbsr* g, int tau, btc_stream_t stream, unsigned long
  * the device.  The caller passes the Bit-BSR (reference layout, e.g. from
  * btc_bitbsr_info or btc_convert_*) and a device word d_out for the count (NULL: use
  * bcsr->result).  The count kernel's scratch (one partial sum per CTA plus a completion
- * counter) is a fixed array inside the library's device image: 2048 partial-sum slots,
- * 16,392 bytes, held by every GPU that loads the library until the process exits.  A GPU
+ * counter) is a fixed array inside the library's device image: 2048 partial-sum slots
+ * and two control words, 16,400 bytes, held by every GPU that loads the library until the process exits.  A GPU
  * whose count grid needs more than 2048 CTAs is rejected with BTC_E_INVAL and a message
  * on stderr (a B200 needs 592).  The first call on each device looks up the array's
  * device address (cudaGetSymbolAddress) with that device current; make that first call
