@@ -45,6 +45,12 @@ EXPORTS = [
     "btc_strerror",
     "btc_abi_version",
     "btc_count_bcsr_noalloc",
+    "btc_batch_build",
+    "btc_batch_rebuild",
+    "btc_batch_count",
+    "btc_batch_info",
+    "btc_batch_row_offsets",
+    "btc_batch_free",
 ]
 
 
@@ -119,8 +125,15 @@ def lib():
         L.btc_strerror.restype = C.c_char_p
         L.btc_abi_version.argtypes = []
         L.btc_count_bcsr_noalloc.argtypes = [P(BtcBcsrDevice), C.c_int, C.c_int, vp, vp]
+        L.btc_batch_build.argtypes = [vp, vp, vp, vp, i32, C.c_int, u32, vp, P(vp)]
+        L.btc_batch_rebuild.argtypes = [vp, vp, vp, vp, vp, i32, C.c_int, u32, vp]
+        L.btc_batch_count.argtypes = [vp, C.c_int, vp, vp, vp]
+        L.btc_batch_info.argtypes = [vp, P(BtcBitbsrView)]
+        L.btc_batch_row_offsets.argtypes = [vp, vp]
+        L.btc_batch_free.argtypes = [vp]
+        L.btc_batch_free.restype = None
         for name in EXPORTS:
-            if name not in ("btc_bcsr_free", "btc_free", "btc_strerror"):
+            if name not in ("btc_bcsr_free", "btc_free", "btc_strerror", "btc_batch_free"):
                 getattr(L, name).restype = C.c_int
         _L = L
     return _L

@@ -31,6 +31,7 @@ __all__ = [
     "convert_coo_to_bcsr_16x128_gpu", "convert_coo_to_bcsr_16x32_gpu",
     "count_triangles_16x128_adaptive", "count_triangles_16x32_adaptive",
     "preprocess_for_triangle_counting", "lite_select_tile_cols", "BitBSR", "default_tau",
+    "Batch",
 ]
 
 
@@ -323,6 +324,90 @@ class BitBSR:
     def free(self) -> None:
         if self._h:
             lib().btc_free(self._h)
+            self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many graphs in one Bit-BSR build and one count launch (btc_batch_*).
+
+    graphs: list of (src, dst, n) with local vertex ids; or pass concatenated arrays
+    with ``offsets`` (num_graphs+1) and ``num_vertices``.  Arrays may be numpy (host) or
+    torch CUDA int32 tensors."""
+
+    def __init__(self, graphs=None, tile_cols: int = 0, stream=None, *, src=None, dst=None,
+                 offsets=None, num_vertices=None):
+        self._h = C.c_void_p(None)
+        self._build(lib().btc_batch_build, graphs, tile_cols, stream, src, dst, offsets,
+                    num_vertices, first=True)
+
+    @staticmethod
+    def concat(graphs):
+        srcs = [np.asarray(s, np.int32) for s, _, _ in graphs]
+        dsts = [np.asarray(d, np.int32) for _, d, _ in graphs]
+        offsets = np.zeros(len(graphs) + 1, np.int64)
+        offsets[1:] = np.cumsum([len(s) for s in srcs])
+        nv = np.array([n for _, _, n in graphs], np.int32)
+        src = np.concatenate(srcs) if srcs else np.zeros(0, np.int32)
+        dst = np.concatenate(dsts) if dsts else np.zeros(0, np.int32)
+        return src, dst, offsets, nv
+
+    def _build(self, fn, graphs, tile_cols, stream, src, dst, offsets, num_vertices, first):
+        if graphs is not None:
+            src, dst, offsets, num_vertices = Batch.concat(graphs)
+        offsets = np.ascontiguousarray(offsets, np.int64)
+        num_vertices = np.ascontiguousarray(num_vertices, np.int32)
+        sp, dp, m, flags, keep = _edge_ptrs(src, dst)
+        if m != int(offsets[-1]):
+            raise BtcError(_lib.BTC_E_INVAL, "offsets[-1] != number of edges")
+        self.num_graphs = len(num_vertices)
+        args = [sp, dp, offsets.ctypes.data, num_vertices.ctypes.data, self.num_graphs,
+                int(tile_cols), flags, _stream_ptr(stream)]
+        if first:
+            check(fn(*args, C.byref(self._h)), "btc_batch_build")
+        else:
+            check(fn(self._h, *args), "btc_batch_rebuild")
+        del keep
+
+    def rebuild(self, graphs=None, tile_cols: int = 0, stream=None, *, src=None, dst=None,
+                offsets=None, num_vertices=None) -> None:
+        self._build(lib().btc_batch_rebuild, graphs, tile_cols, stream, src, dst, offsets,
+                    num_vertices, first=False)
+
+    def count(self, tau: int = _lib.BTC_TAU_DEFAULT, stream=None) -> np.ndarray:
+        """Per-graph triangle counts (uint64 numpy array); waits for them."""
+        out = np.zeros(self.num_graphs, np.uint64)
+        check(lib().btc_batch_count(self._h, int(tau), _stream_ptr(stream), None,
+                                    out.ctypes.data), "btc_batch_count")
+        return out
+
+    def count_async(self, d_counts: int, tau: int = _lib.BTC_TAU_DEFAULT, stream=None) -> None:
+        """Counts into device memory d_counts (num_graphs uint64) without waiting."""
+        check(lib().btc_batch_count(self._h, int(tau), _stream_ptr(stream), d_counts, None),
+              "btc_batch_count")
+
+    def info(self) -> _lib.BtcBitbsrView:
+        v = _lib.BtcBitbsrView()
+        check(lib().btc_batch_info(self._h, C.byref(v)), "btc_batch_info")
+        return v
+
+    def row_offsets(self) -> np.ndarray:
+        out = np.zeros(self.num_graphs + 1, np.uint32)
+        check(lib().btc_batch_row_offsets(self._h, out.ctypes.data), "btc_batch_row_offsets")
+        return out
+
+    def to_host(self) -> dict:
+        v = self.info()
+        return _copy_out(v.bcsr, int(v.tile_cols))
+
+    def free(self) -> None:
+        if self._h:
+            lib().btc_batch_free(self._h)
             self._h = C.c_void_p(None)
 
     def __del__(self):

@@ -174,3 +174,65 @@ def write_bin_csr(path: str, rowptr, col, n: int):
         rowptr.tofile(f)
         col.tofile(f)
         np.ones(len(col), np.float32).tofile(f)
+
+
+def union_graph(graphs):
+    """Block-diagonal union of graphs, laid out as a batch lays them out: graph g's
+    vertex v becomes 16 * (row blocks of graphs before g) + v."""
+    srcs, dsts = [], []
+    base = 0
+    for s, d, n in graphs:
+        srcs.append(np.asarray(s, np.int64) + base)
+        dsts.append(np.asarray(d, np.int64) + base)
+        base += 16 * ((n + 15) // 16)
+    src = np.concatenate(srcs).astype(np.int32) if srcs else np.zeros(0, np.int32)
+    dst = np.concatenate(dsts).astype(np.int32) if dsts else np.zeros(0, np.int32)
+    return src, dst, base
+
+
+def batch_mix(num_graphs: int, n_min: int = 256, n_max: int = 65536, seed: int = 0):
+    """The mixed batch workload: vertex counts log-uniform in [n_min, n_max]; each graph
+    (seeded per graph) is Erdos-Renyi with mean degree U[8, 32], an 8-community SBM with
+    p_in U[0.05, 0.3] and p_out 0.001, or R-MAT with scale U{10..16} and edge factor 8,
+    chosen uniformly.  Edges are raw draws: duplicates and self-loops are kept (the
+    builder removes them) so that generation stays cheap.  R-MAT graphs take their
+    vertex count from their scale.  Returns a list of (src, dst, n, kind)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for g in range(num_graphs):
+        gr = np.random.default_rng((seed, g))
+        kind = int(rng.integers(0, 3))
+        n = int(round(np.exp(rng.uniform(np.log(n_min), np.log(n_max)))))
+        if kind == 0:
+            d = rng.uniform(8, 32)
+            m = int(round(n * d / 2))
+            src = gr.integers(0, n, m, dtype=np.int32)
+            dst = gr.integers(0, n, m, dtype=np.int32)
+            out.append((src, dst, n, "er"))
+        elif kind == 1:
+            p_in = rng.uniform(0.05, 0.3)
+            bounds = np.linspace(0, n, 9).astype(np.int64)
+            us, vs = [], []
+            for i in range(8):
+                for j in range(i, 8):
+                    ni, nj = bounds[i + 1] - bounds[i], bounds[j + 1] - bounds[j]
+                    pairs = ni * (ni - 1) // 2 if i == j else ni * nj
+                    k = gr.binomial(pairs, p_in if i == j else 0.001) if pairs > 0 else 0
+                    if k:
+                        us.append(gr.integers(bounds[i], bounds[i + 1], k, dtype=np.int64))
+                        vs.append(gr.integers(bounds[j], bounds[j + 1], k, dtype=np.int64))
+            src = np.concatenate(us).astype(np.int32) if us else np.zeros(0, np.int32)
+            dst = np.concatenate(vs).astype(np.int32) if vs else np.zeros(0, np.int32)
+            out.append((src, dst, n, "sbm"))
+        else:
+            scale = int(rng.integers(10, 17))
+            n = 1 << scale
+            m = 8 << scale
+            u = np.zeros(m, np.int64)
+            v = np.zeros(m, np.int64)
+            for _ in range(scale):
+                r = gr.random(m, dtype=np.float32)
+                u = (u << 1) | (r >= 0.76)
+                v = (v << 1) | (((r >= 0.57) & (r < 0.76)) | (r >= 0.95))
+            out.append((u.astype(np.int32), v.astype(np.int32), n, "rmat"))
+    return out

@@ -1,0 +1,447 @@
+// batch.cu -- many graphs in one build and one persistent count launch.
+//
+// A batch is the block-diagonal union of its graphs: graph g's local vertex v becomes
+// global vertex V_g + v with V_g = 16 * (row blocks of graphs 0..g-1), so every row block
+// belongs to exactly one graph and no tile holds edges of two graphs.  The union's
+// Bit-BSR is the reference layout and the count kernel runs on it unchanged; it adds each
+// tile's sum to the graph owning the tile's row block (k_count's graph attribution).
+//
+// The cell bitmap is segmented: graph g has its own R_g x ceil(ncb_g/32)-word grid over
+// the column blocks its vertices touch, so the bitmap grows with the sum of the graphs'
+// squared sizes, not with the square of the batch's total vertex count.  Build passes are
+// those of bitmap.cu (mark, count, scan, emit, fill), with the graph of an edge found by
+// a binary search over the edge offsets and the graph of a bitmap word by a search over
+// the segment offsets.
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "common.cuh"
+#include "handle.cuh"
+
+namespace btc200 {
+
+struct GraphSeg {
+    uint32_t row_off;  // first global row block
+    int32_t n;         // vertices (local ids are in [0, n))
+    uint32_t vbase;    // first global vertex id (16 * row_off)
+    uint32_t cb_lo;    // first global column block of the graph's vertex range
+    uint32_t wpr;      // bitmap words per row block
+    uint32_t pad;
+    uint64_t bm_off;   // first bitmap word of the graph
+};
+
+namespace bt {
+
+constexpr int kThreads = 256;
+constexpr int kWordsPerThread = 16;
+constexpr int kChunk = kThreads * kWordsPerThread;
+
+// last g in [0, G) with off[g] <= x (off[0] == 0; equal offsets are empty graphs)
+template <class T>
+__device__ __forceinline__ uint32_t last_le(const T* __restrict__ off, uint32_t G, T x)
+{
+    uint32_t lo = 0, hi = G;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (off[mid] <= x) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Orients edge i of its graph to local (r, c), r > c.  false: self-loop or bad id.
+__device__ __forceinline__ bool local_edge(const int32_t* __restrict__ src,
+                                           const int32_t* __restrict__ dst, int64_t i,
+                                           const GraphSeg& s, uint32_t& r, uint32_t& c, bool& bad)
+{
+    const int32_t u = src[i], v = dst[i];
+    bad = (u < 0) | (v < 0) | (u >= s.n) | (v >= s.n);
+    if (bad || u == v) return false;
+    r = (uint32_t)max(u, v);
+    c = (uint32_t)min(u, v);
+    return true;
+}
+
+template <int LOG2C>
+__device__ __forceinline__ uint64_t cell_word(const GraphSeg& s, uint32_t r, uint32_t c,
+                                              uint32_t& bit)
+{
+    const uint32_t cb = ((s.vbase + c) >> LOG2C) - s.cb_lo;
+    bit = 1u << (cb & 31u);
+    return s.bm_off + (uint64_t)(r >> 4) * s.wpr + (cb >> 5);
+}
+
+template <int LOG2C>
+__global__ void __launch_bounds__(kThreads)
+k_mark_b(const int32_t* __restrict__ src, const int32_t* __restrict__ dst, int64_t m,
+         const GraphSeg* __restrict__ segs, const int64_t* __restrict__ e_off, uint32_t G,
+         uint32_t* bitmap, unsigned long long* __restrict__ bad_count)
+{
+    uint32_t nbad = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const GraphSeg s = segs[last_le<int64_t>(e_off, G, i)];
+        uint32_t r, c, bit;
+        bool bad;
+        if (local_edge(src, dst, i, s, r, c, bad)) {
+            const uint64_t w = cell_word<LOG2C>(s, r, c, bit);
+            if (!(bitmap[w] & bit)) atomicOr(&bitmap[w], bit);
+        }
+        nbad += bad;
+    }
+    nbad = __reduce_add_sync(kFull, nbad);
+    if ((threadIdx.x & 31) == 0 && nbad) atomicAdd(bad_count, (unsigned long long)nbad);
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_emit_b(const uint32_t* __restrict__ bitmap, uint64_t W, const GraphSeg* __restrict__ segs,
+         const uint64_t* __restrict__ bm_off, uint32_t G, const uint32_t* __restrict__ chunk_base,
+         uint32_t* __restrict__ prefix, uint32_t* __restrict__ indices,
+         uint32_t* __restrict__ row_indices, uint32_t* __restrict__ indptr)
+{
+    __shared__ uint32_t s_warp[kThreads / kWarp];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t w0 = (uint64_t)blockIdx.x * kChunk + (uint64_t)threadIdx.x * kWordsPerThread;
+    uint32_t x[kWordsPerThread];
+#pragma unroll
+    for (int k = 0; k < kWordsPerThread; ++k) x[k] = (w0 + k < W) ? bitmap[w0 + k] : 0u;
+    uint32_t mine = 0;
+#pragma unroll
+    for (int k = 0; k < kWordsPerThread; ++k) mine += __popc(x[k]);
+    uint32_t incl = mine;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t t = __shfl_up_sync(kFull, incl, d);
+        if (lane >= d) incl += t;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    uint32_t base = chunk_base[blockIdx.x] + incl - mine;
+#pragma unroll
+    for (int w = 0; w < kThreads / kWarp; ++w) base += (w < warp) ? s_warp[w] : 0u;
+    if (w0 >= W) return;
+
+    uint32_t g = last_le<uint64_t>(bm_off, G, w0);
+    GraphSeg s = segs[g];
+    uint64_t lw = w0 - s.bm_off;
+    uint32_t rb = (uint32_t)(lw / s.wpr);
+    uint32_t cw = (uint32_t)(lw - (uint64_t)rb * s.wpr);
+    for (int k = 0; k < kWordsPerThread; ++k) {
+        const uint64_t w = w0 + k;
+        if (w >= W) break;
+        while (w >= bm_off[g + 1]) {  // next non-empty graph
+            ++g;
+            s = segs[g];
+            rb = 0;
+            cw = 0;
+        }
+        prefix[w] = base;
+        if (cw == 0) indptr[s.row_off + rb] = base;
+        uint32_t bits = x[k];
+        while (bits) {
+            const uint32_t b = __ffs(bits) - 1;
+            bits &= bits - 1;
+            indices[base] = s.cb_lo + cw * 32 + b;
+            row_indices[base] = s.row_off + rb;
+            ++base;
+        }
+        if (++cw == s.wpr) {
+            cw = 0;
+            ++rb;
+        }
+    }
+}
+
+template <int LOG2C>
+__global__ void __launch_bounds__(kThreads)
+k_fill_b(const int32_t* __restrict__ src, const int32_t* __restrict__ dst, int64_t m,
+         const GraphSeg* __restrict__ segs, const int64_t* __restrict__ e_off, uint32_t G,
+         const uint32_t* __restrict__ bitmap, const uint32_t* __restrict__ prefix,
+         uint32_t* __restrict__ blocks)
+{
+    constexpr int C = 1 << LOG2C;
+    constexpr int WPR = C / 32;
+    constexpr int TW = 16 * WPR;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const GraphSeg s = segs[last_le<int64_t>(e_off, G, i)];
+        uint32_t r, c, bit;
+        bool bad;
+        if (!local_edge(src, dst, i, s, r, c, bad)) continue;
+        const uint64_t w = cell_word<LOG2C>(s, r, c, bit);
+        const uint32_t t = prefix[w] + __popc(bitmap[w] & (bit - 1u));
+        const uint32_t cl = (s.vbase + c) & (C - 1);
+        atomicOr(&blocks[(size_t)t * TW + (r & 15u) * WPR + (cl >> 5)], 1u << (cl & 31u));
+    }
+}
+
+__global__ void k_set_last_b(uint32_t* __restrict__ indptr, uint32_t R,
+                             const unsigned long long* __restrict__ total)
+{
+    indptr[R] = (uint32_t)*total;
+}
+
+}  // namespace bt
+
+int grid_for(int64_t work, int threads);
+int launch_tile_scan(uint32_t* per_tile, uint32_t ntiles, unsigned long long* total, cudaStream_t s);
+int launch_bitmap_count(const uint32_t* bitmap, uint64_t W, uint32_t* chunk_count, cudaStream_t s);
+
+}  // namespace btc200
+
+using namespace btc200;
+
+struct btc_batch {
+    btc_bitbsr g;  // the union graph's Bit-BSR, workspace and count scratch
+    int32_t num_graphs = 0;
+    DevBuf segs, e_off, bm_off, row_off, counts;
+    std::vector<GraphSeg> h_segs;
+    std::vector<int64_t> h_eoff;
+    std::vector<uint64_t> h_bmoff;
+    std::vector<uint32_t> h_rowoff;
+    void release()
+    {
+        g.release_all();
+        segs.release();
+        e_off.release();
+        bm_off.release();
+        row_off.release();
+        counts.release();
+    }
+};
+
+static int batch_build_into(btc_batch* b, const int32_t* src, const int32_t* dst,
+                            const int64_t* edge_offsets, const int32_t* num_vertices, int32_t G,
+                            int tile_cols, uint32_t flags, cudaStream_t s)
+{
+    if (G < 1 || !edge_offsets || !num_vertices) return BTC_E_INVAL;
+    if (flags & ~BTC_INPUT_ON_HOST) return BTC_E_INVAL;
+    const int64_t m = edge_offsets[G];
+    if (edge_offsets[0] != 0 || m < 0 || (uint64_t)m > (1ull << 32) - (uint64_t)kSortTile)
+        return BTC_E_INVAL;
+    if (m > 0 && (!src || !dst)) return BTC_E_INVAL;
+    int64_t n_sum = 0;
+    for (int32_t i = 0; i < G; ++i) {
+        if (num_vertices[i] < 0 || edge_offsets[i + 1] < edge_offsets[i]) return BTC_E_INVAL;
+        n_sum += num_vertices[i];
+    }
+    if (tile_cols == 0) tile_cols = btc_lite_select_tile_cols(m, (int32_t)(n_sum > 0x7fffffff ? 0x7fffffff : n_sum), 0);
+    if (tile_cols != 32 && tile_cols != 128) return BTC_E_INVAL;
+    const int log2c = tile_cols == 128 ? 7 : 5;
+
+    // ---- host geometry ----------------------------------------------------------
+    b->num_graphs = G;
+    b->h_segs.resize((size_t)G);
+    b->h_eoff.assign(edge_offsets, edge_offsets + G + 1);
+    b->h_bmoff.resize((size_t)G + 1);
+    b->h_rowoff.resize((size_t)G + 1);
+    uint64_t rows = 0, words = 0;
+    for (int32_t i = 0; i < G; ++i) {
+        GraphSeg& sg = b->h_segs[(size_t)i];
+        const uint64_t Ri = ((uint64_t)num_vertices[i] + 15) / 16;
+        sg.row_off = (uint32_t)rows;
+        sg.n = num_vertices[i];
+        sg.vbase = (uint32_t)(rows * 16);
+        sg.cb_lo = (uint32_t)((rows * 16) >> log2c);
+        const uint64_t hi = num_vertices[i] > 0 ? ((rows * 16 + num_vertices[i] - 1) >> log2c) : sg.cb_lo;
+        const uint64_t ncb = hi - sg.cb_lo + 1;
+        sg.wpr = (uint32_t)((ncb + 31) / 32);
+        sg.pad = 0;
+        sg.bm_off = words;
+        b->h_rowoff[(size_t)i] = (uint32_t)rows;
+        b->h_bmoff[(size_t)i] = words;
+        rows += Ri;
+        words += Ri * sg.wpr;
+        if (rows * 16 > 0x7fffffffull) return BTC_E_INVAL;
+    }
+    b->h_rowoff[(size_t)G] = (uint32_t)rows;
+    b->h_bmoff[(size_t)G] = words;
+    if (words * 8 > (4ull << 30)) return BTC_E_INVAL;  // bitmap + prefix budget
+
+    btc_bitbsr* g = &b->g;
+    BTC_CUDA_TRY(cudaGetDevice(&g->device));
+    g->tile_cols = tile_cols;
+    g->n = (int32_t)(rows * 16);
+    g->n_row_blocks = (int32_t)rows;
+    g->input_edges = m;
+    g->edges_known = false;
+    if (!g->h_meta) {
+        void* p = nullptr;
+        if (cudaMallocHost(&p, sizeof(unsigned long long) * kMetaSlots) != cudaSuccess) {
+            cudaGetLastError();
+            return BTC_E_NOMEM;
+        }
+        g->h_meta = static_cast<unsigned long long*>(p);
+    }
+    BTC_TRY(g->meta.reserve(sizeof(unsigned long long) * kMetaSlots));
+    unsigned long long* meta = g->meta.as<unsigned long long>();
+    BTC_CUDA_TRY(cudaMemsetAsync(meta, 0, sizeof(unsigned long long) * kMetaSlots, s));
+
+    BTC_TRY(b->segs.reserve(sizeof(GraphSeg) * (size_t)G));
+    BTC_TRY(b->e_off.reserve(sizeof(int64_t) * ((size_t)G + 1)));
+    BTC_TRY(b->bm_off.reserve(sizeof(uint64_t) * ((size_t)G + 1)));
+    BTC_TRY(b->row_off.reserve(sizeof(uint32_t) * ((size_t)G + 1)));
+    // pageable sources: the copies are staged before cudaMemcpyAsync returns
+    BTC_CUDA_TRY(cudaMemcpyAsync(b->segs.ptr, b->h_segs.data(), sizeof(GraphSeg) * (size_t)G,
+                                 cudaMemcpyHostToDevice, s));
+    BTC_CUDA_TRY(cudaMemcpyAsync(b->e_off.ptr, b->h_eoff.data(), sizeof(int64_t) * ((size_t)G + 1),
+                                 cudaMemcpyHostToDevice, s));
+    BTC_CUDA_TRY(cudaMemcpyAsync(b->bm_off.ptr, b->h_bmoff.data(),
+                                 sizeof(uint64_t) * ((size_t)G + 1), cudaMemcpyHostToDevice, s));
+    BTC_CUDA_TRY(cudaMemcpyAsync(b->row_off.ptr, b->h_rowoff.data(),
+                                 sizeof(uint32_t) * ((size_t)G + 1), cudaMemcpyHostToDevice, s));
+
+    const int32_t* d_src = src;
+    const int32_t* d_dst = dst;
+    if ((flags & BTC_INPUT_ON_HOST) && m > 0) {
+        BTC_TRY(g->in_src.reserve(sizeof(int32_t) * (size_t)m));
+        BTC_TRY(g->in_dst.reserve(sizeof(int32_t) * (size_t)m));
+        BTC_CUDA_TRY(cudaMemcpyAsync(g->in_src.ptr, src, sizeof(int32_t) * (size_t)m,
+                                     cudaMemcpyHostToDevice, s));
+        BTC_CUDA_TRY(cudaMemcpyAsync(g->in_dst.ptr, dst, sizeof(int32_t) * (size_t)m,
+                                     cudaMemcpyHostToDevice, s));
+        d_src = g->in_src.as<int32_t>();
+        d_dst = g->in_dst.as<int32_t>();
+    }
+
+    // ---- mark, count, scan ----------------------------------------------------------
+    const size_t chunks = (size_t)((words + bt::kChunk - 1) / bt::kChunk);
+    BTC_TRY(g->bitmap.reserve(sizeof(uint32_t) * (words ? words : 1)));
+    BTC_TRY(g->prefix.reserve(sizeof(uint32_t) * (words ? words : 1)));
+    BTC_TRY(g->tile_base.reserve(sizeof(uint32_t) * (chunks + 1)));
+    const GraphSeg* dsegs = b->segs.as<GraphSeg>();
+    const int64_t* deoff = b->e_off.as<int64_t>();
+    const int egrid = grid_for((m + 3) / 4, bt::kThreads);
+    if (words) {
+        BTC_CUDA_TRY(cudaMemsetAsync(g->bitmap.ptr, 0, sizeof(uint32_t) * words, s));
+        if (m > 0) {
+            if (tile_cols == 128)
+                bt::k_mark_b<7><<<egrid, bt::kThreads, 0, s>>>(d_src, d_dst, m, dsegs, deoff,
+                                                               (uint32_t)G, g->bitmap.as<uint32_t>(),
+                                                               meta + kMetaBad);
+            else
+                bt::k_mark_b<5><<<egrid, bt::kThreads, 0, s>>>(d_src, d_dst, m, dsegs, deoff,
+                                                               (uint32_t)G, g->bitmap.as<uint32_t>(),
+                                                               meta + kMetaBad);
+        }
+        BTC_TRY(launch_bitmap_count(g->bitmap.as<uint32_t>(), words, g->tile_base.as<uint32_t>(), s));
+        BTC_TRY(launch_tile_scan(g->tile_base.as<uint32_t>(), (uint32_t)chunks, meta + kMetaTiles, s));
+    } else if (m > 0) {
+        // only empty graphs: every edge has an out-of-range id
+        return BTC_E_RANGE;
+    }
+    BTC_CUDA_TRY(cudaMemcpyAsync(g->h_meta, meta, sizeof(unsigned long long) * 3,
+                                 cudaMemcpyDeviceToHost, s));
+    BTC_CUDA_TRY(cudaStreamSynchronize(s));
+    if (g->h_meta[kMetaBad] != 0) return BTC_E_RANGE;
+    const unsigned long long tiles = g->h_meta[kMetaTiles];
+    if (tiles > 0xffffffffull) return BTC_E_INVAL;
+    g->num_tiles = (uint32_t)tiles;
+
+    // ---- tiles ------------------------------------------------------------------
+    const size_t TW = (size_t)16 * (tile_cols / 32);
+    BTC_TRY(g->indptr.reserve(sizeof(uint32_t) * ((size_t)rows + 1)));
+    BTC_TRY(g->indices.reserve(sizeof(uint32_t) * (tiles ? tiles : 1)));
+    BTC_TRY(g->row_indices.reserve(sizeof(uint32_t) * (tiles ? tiles : 1)));
+    BTC_TRY(g->blocks.reserve(sizeof(uint32_t) * TW * (tiles ? tiles : 1)));
+    BTC_TRY(ensure_count_scratch(g));
+    BTC_TRY(b->counts.reserve(sizeof(unsigned long long) * (size_t)G));
+    if (tiles) BTC_CUDA_TRY(cudaMemsetAsync(g->blocks.ptr, 0, sizeof(uint32_t) * TW * tiles, s));
+    if (words)
+        bt::k_emit_b<<<(unsigned)chunks, bt::kThreads, 0, s>>>(
+            g->bitmap.as<uint32_t>(), words, dsegs, b->bm_off.as<uint64_t>(), (uint32_t)G,
+            g->tile_base.as<uint32_t>(), g->prefix.as<uint32_t>(), g->indices.as<uint32_t>(),
+            g->row_indices.as<uint32_t>(), g->indptr.as<uint32_t>());
+    bt::k_set_last_b<<<1, 1, 0, s>>>(g->indptr.as<uint32_t>(), (uint32_t)rows, meta + kMetaTiles);
+    if (m > 0 && words) {
+        if (tile_cols == 128)
+            bt::k_fill_b<7><<<egrid, bt::kThreads, 0, s>>>(d_src, d_dst, m, dsegs, deoff, (uint32_t)G,
+                                                           g->bitmap.as<uint32_t>(),
+                                                           g->prefix.as<uint32_t>(),
+                                                           g->blocks.as<uint32_t>());
+        else
+            bt::k_fill_b<5><<<egrid, bt::kThreads, 0, s>>>(d_src, d_dst, m, dsegs, deoff, (uint32_t)G,
+                                                           g->bitmap.as<uint32_t>(),
+                                                           g->prefix.as<uint32_t>(),
+                                                           g->blocks.as<uint32_t>());
+    }
+    return cudaGetLastError() == cudaSuccess ? BTC_OK : BTC_E_CUDA;
+}
+
+extern "C" {
+
+int btc_batch_build(const int32_t* src, const int32_t* dst, const int64_t* edge_offsets,
+                    const int32_t* num_vertices, int32_t num_graphs, int tile_cols, uint32_t flags,
+                    btc_stream_t stream, btc_batch** out)
+{
+    if (!out) return BTC_E_INVAL;
+    *out = nullptr;
+    btc_batch* b = new (std::nothrow) btc_batch();
+    if (!b) return BTC_E_NOMEM;
+    const int st = batch_build_into(b, src, dst, edge_offsets, num_vertices, num_graphs, tile_cols,
+                                    flags, stream);
+    if (st != BTC_OK) {
+        b->release();
+        delete b;
+        return st;
+    }
+    *out = b;
+    return BTC_OK;
+}
+
+int btc_batch_rebuild(btc_batch* b, const int32_t* src, const int32_t* dst,
+                      const int64_t* edge_offsets, const int32_t* num_vertices, int32_t num_graphs,
+                      int tile_cols, uint32_t flags, btc_stream_t stream)
+{
+    if (!b) return BTC_E_INVAL;
+    return batch_build_into(b, src, dst, edge_offsets, num_vertices, num_graphs, tile_cols, flags,
+                            stream);
+}
+
+int btc_batch_count(btc_batch* b, int tau, btc_stream_t stream, unsigned long long* d_counts,
+                    unsigned long long* h_counts)
+{
+    if (!b) return BTC_E_INVAL;
+    btc_bitbsr* g = &b->g;
+    if (tau == BTC_TAU_DEFAULT) tau = default_tau(g->tile_cols);
+    if (tau < 0) return BTC_E_INVAL;
+    BTC_TRY(ensure_count_scratch(g));
+    unsigned long long* counts = d_counts ? d_counts : b->counts.as<unsigned long long>();
+    const size_t bytes = sizeof(unsigned long long) * (size_t)b->num_graphs;
+    BTC_CUDA_TRY(cudaMemsetAsync(counts, 0, bytes, stream));
+    CountScratch scr{g->partials.as<unsigned long long>(), g->done.as<unsigned int>(),
+                     reinterpret_cast<unsigned long long*>(g->done.as<char>() + 8),
+                     g->result.as<unsigned long long>(), nullptr};
+    BTC_TRY(launch_count(g->tile_cols, g->indptr.as<uint32_t>(), g->indices.as<uint32_t>(),
+                         g->row_indices.as<uint32_t>(), g->blocks.as<uint32_t>(), g->num_tiles,
+                         g->n_row_blocks, tau, scr, stream, b->row_off.as<uint32_t>(),
+                         (uint32_t)b->num_graphs, counts));
+    if (h_counts) {
+        BTC_CUDA_TRY(cudaMemcpyAsync(h_counts, counts, bytes, cudaMemcpyDeviceToHost, stream));
+        BTC_CUDA_TRY(cudaStreamSynchronize(stream));
+    }
+    return BTC_OK;
+}
+
+int btc_batch_info(const btc_batch* b, btc_bitbsr_view* v)
+{
+    if (!b) return BTC_E_INVAL;
+    return btc_bitbsr_info(&b->g, v);
+}
+
+int btc_batch_row_offsets(const btc_batch* b, uint32_t* row_offsets)
+{
+    if (!b || !row_offsets) return BTC_E_INVAL;
+    std::memcpy(row_offsets, b->h_rowoff.data(), sizeof(uint32_t) * ((size_t)b->num_graphs + 1));
+    return BTC_OK;
+}
+
+void btc_batch_free(btc_batch* b)
+{
+    if (!b) return;
+    b->release();
+    delete b;
+}
+
+}  // extern "C"

@@ -335,3 +335,11 @@ int launch_popcount_sum(int tile_cols, const uint32_t* blocks, uint64_t num_tile
 }
 
 }  // namespace btc200
+
+namespace btc200 {
+int launch_bitmap_count(const uint32_t* bitmap, uint64_t W, uint32_t* chunk_count, cudaStream_t s)
+{
+    if (W) bm::k_bm_count<<<(unsigned)bitmap_chunks(W), bm::kThreads, 0, s>>>(bitmap, W, chunk_count);
+    return cudaGetLastError() == cudaSuccess ? BTC_OK : BTC_E_CUDA;
+}
+}  // namespace btc200

@@ -8,6 +8,7 @@
 #include <new>
 
 #include "common.cuh"
+#include "handle.cuh"
 
 namespace btc200 {
 
@@ -60,53 +61,11 @@ using namespace btc200;
 
 // Engine's default dense/sparse switch.  A tile takes the binary tensor-core path
 // when its popcount exceeds tau.
-static int default_tau(int tile_cols) { return tile_cols == 128 ? 512 : 64; }
+int default_tau(int tile_cols) { return tile_cols == 128 ? 512 : 64; }
 
 static constexpr uint64_t kMaxEdges = (1ull << 32) - (uint64_t)kSortTile;
 
-struct btc_bitbsr {
-    int device = 0;
-    int tile_cols = 0;
-    int32_t n = 0;
-    int32_t n_row_blocks = 0;
-    uint32_t num_tiles = 0;
-    int64_t input_edges = 0;
-    // Bit-BSR arrays (reference layout)
-    DevBuf indptr, indices, row_indices, blocks, result;
-    // build workspace
-    DevBuf in_src, in_dst, keys0, keys1, sort_scratch, tile_base, meta, deg, rank, bitmap, prefix;
-    bool used_bitmap = false;
-    // count scratch
-    DevBuf partials, done;
-    unsigned long long* h_meta = nullptr;  // pinned, 8 slots
-    bool edges_known = false;
-    int64_t num_edges = 0;
-
-    size_t device_bytes() const
-    {
-        const DevBuf* all[] = {&indptr, &indices, &row_indices, &blocks, &result, &in_src, &in_dst,
-                               &keys0, &keys1, &sort_scratch, &tile_base, &meta, &deg, &rank,
-                               &bitmap, &prefix, &partials, &done};
-        size_t s = 0;
-        for (const DevBuf* b : all) s += b->bytes;
-        return s;
-    }
-    void release_all()
-    {
-        DevBuf* all[] = {&indptr, &indices, &row_indices, &blocks, &result, &in_src, &in_dst,
-                         &keys0, &keys1, &sort_scratch, &tile_base, &meta, &deg, &rank,
-                         &bitmap, &prefix, &partials, &done};
-        for (DevBuf* b : all) b->release();
-        if (h_meta) cudaFreeHost(h_meta);
-        h_meta = nullptr;
-    }
-};
-
-// meta slots (device uint64): 0 valid edges, 1 out-of-range ids, 2 tiles, 3 unique
-// edges, 4 vertex count for the degree sort
-enum { kMetaValid = 0, kMetaBad = 1, kMetaTiles = 2, kMetaUniq = 3, kMetaN = 4, kMetaSlots = 8 };
-
-static int ensure_count_scratch(btc_bitbsr* g)
+int ensure_count_scratch(btc_bitbsr* g)
 {
     const int grid = count_grid_size(128) > count_grid_size(32) ? count_grid_size(128)
                                                                  : count_grid_size(32);
@@ -260,7 +219,7 @@ static int build_into(btc_bitbsr* g, const int32_t* src, const int32_t* dst, int
     return BTC_OK;
 }
 
-static int count_handle(btc_bitbsr* g, int tau, cudaStream_t s, unsigned long long* d_out2)
+int count_handle(btc_bitbsr* g, int tau, cudaStream_t s, unsigned long long* d_out2)
 {
     if (!g) return BTC_E_INVAL;
     if (tau == BTC_TAU_DEFAULT) tau = default_tau(g->tile_cols);
@@ -269,10 +228,9 @@ static int count_handle(btc_bitbsr* g, int tau, cudaStream_t s, unsigned long lo
     CountScratch scr{g->partials.as<unsigned long long>(), g->done.as<unsigned int>(),
                      reinterpret_cast<unsigned long long*>(g->done.as<char>() + 8),
                      g->result.as<unsigned long long>(), d_out2};
-    const int64_t ncb = ((int64_t)g->n + g->tile_cols - 1) / g->tile_cols;
     return launch_count(g->tile_cols, g->indptr.as<uint32_t>(), g->indices.as<uint32_t>(),
                         g->row_indices.as<uint32_t>(), g->blocks.as<uint32_t>(), g->num_tiles,
-                        g->n_row_blocks, ncb, tau, scr, s);
+                        g->n_row_blocks, tau, scr, s);
 }
 
 // ===========================================================================
@@ -523,9 +481,8 @@ static int count_struct(btc_bcsr_device* b, int tile_cols, float* kernel_ms,
     CountScratch scr{ss.partials[dev].as<unsigned long long>(), ss.done[dev].as<unsigned int>(),
                      reinterpret_cast<unsigned long long*>(ss.done[dev].as<char>() + 8), b->result,
                      nullptr};
-    const int64_t ncb = ((int64_t)b->n + tile_cols - 1) / tile_cols;
     int st = launch_count(tile_cols, b->indptr, b->indices, b->row_indices, b->blocks, b->num_blocks,
-                          b->n_row_blocks, ncb, default_tau(tile_cols), scr, nullptr);
+                          b->n_row_blocks, default_tau(tile_cols), scr, nullptr);
     if (st == BTC_OK && kernel_ms && cudaEventRecord(e1, nullptr) != cudaSuccess) st = BTC_E_CUDA;
     if (st == BTC_OK && cudaMemcpy(out, b->result, sizeof(unsigned long long),
                                    cudaMemcpyDeviceToHost) != cudaSuccess)

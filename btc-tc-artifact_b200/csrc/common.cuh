@@ -143,10 +143,14 @@ struct CountScratch {
 };
 
 int count_grid_size(int tile_cols);
+// graph_rows / graph_counts (nullable): per-graph attribution for batches; graph g
+// owns row blocks [graph_rows[g], graph_rows[g+1]) and its count is added to
+// graph_counts[g] (which the caller zeroes).
 int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
                  const uint32_t* row_indices, const uint32_t* blocks, uint32_t num_tiles,
-                 int32_t n_row_blocks, int64_t n_col_blocks, int tau, CountScratch scr,
-                 cudaStream_t s);
+                 int32_t n_row_blocks, int tau, CountScratch scr, cudaStream_t s,
+                 const uint32_t* graph_rows = nullptr, uint32_t num_graphs = 0,
+                 unsigned long long* graph_counts = nullptr);
 
 // Queue/completion words of the count kernel: done (u32) at byte 0, work (u64) at 8.
 constexpr size_t kCountCtlBytes = 16;

@@ -11,8 +11,8 @@
 // Work mapping (persistent grid; each warp takes runs of consecutive tiles from a
 // global queue, so the tiles of one row block usually stay with one warp):
 //  * Row block I's column-block list is staged once per row block, as a shared-memory
-//    bitmap with per-word prefix counts (membership and rank in O(1)) when the graph has
-//    at most 8192 column blocks, else as a sorted list (binary search).
+//    bitmap with per-word prefix counts (membership and rank in O(1)) when its column
+//    blocks span at most 8192, else as a sorted list (binary search).
 //  * S is loaded once (one 8-byte load per lane for 16x128); its popcount picks the
 //    path: > tau -> binary tensor core, else CUDA cores.
 //  * The row blocks J_out = J_L*(C/16) + j are consecutive, so their index lists form
@@ -69,6 +69,7 @@ struct __align__(16) WarpSmem {
 struct ARow {
     uint32_t start;  // indptr[I]
     uint32_t len;    // number of tiles in row block I
+    uint32_t base;   // bitmap mode: first column block of the bitmap (multiple of 32)
     uint32_t words;  // bitmap mode: bitmap words in use
     int mode;        // 0: sorted list in shared memory, 1: bitmap, 2: sorted list in HBM
 };
@@ -103,23 +104,25 @@ __device__ __forceinline__ uint32_t slice_of(const uint32_t* S, int r, int j)
 }
 
 // Stages row block I's column-block list for lookups.  Called with the warp converged.
+// The bitmap spans the row block's own column-block range, so it is used whenever
+// that range is at most kBmWords * 32 column blocks wide.
 template <int C>
 __device__ __forceinline__ ARow stage_row(WarpSmem<C>& s, const uint32_t* __restrict__ indptr,
                                           const uint32_t* __restrict__ indices, uint32_t I,
-                                          bool bitmap_ok, int lane)
+                                          int lane)
 {
     ARow A;
     A.start = indptr[I];
     A.len = indptr[I + 1] - A.start;  // >= 1: a tile of row block I is being counted
-    A.words = 0;
+    A.base = indices[A.start] & ~31u;
+    A.words = ((indices[A.start + A.len - 1] - A.base) >> 5) + 1;
     __syncwarp();  // earlier readers of s.a / s.apre are done
-    if (bitmap_ok) {
+    if (A.words <= (uint32_t)kBmWords) {
         A.mode = 1;
-        A.words = (indices[A.start + A.len - 1] >> 5) + 1;  // <= kBmWords
         for (uint32_t w = lane; w < A.words; w += kWarp) s.a.bm[w] = 0u;
         __syncwarp();
         for (uint32_t i = lane; i < A.len; i += kWarp) {
-            const uint32_t k = indices[A.start + i];
+            const uint32_t k = indices[A.start + i] - A.base;
             atomicOr(&s.a.bm[k >> 5], 1u << (k & 31u));
         }
         __syncwarp();
@@ -161,7 +164,8 @@ __device__ __forceinline__ bool a_lookup(const WarpSmem<C>& s, const ARow& A,
                                          uint32_t& pa)
 {
     if (A.mode == 1) {
-        const uint32_t w = b >> 5;
+        if (b < A.base) return false;
+        const uint32_t w = (b - A.base) >> 5;
         if (w >= A.words) return false;
         const uint32_t x = s.a.bm[w];
         const uint32_t bit = 1u << (b & 31u);
@@ -263,12 +267,27 @@ __device__ __forceinline__ unsigned long long bit_pass(WarpSmem<C>& s, uint32_t 
     return acc;
 }
 
+// Adds the warp's partial count to graph g (one atomic per graph change per warp).
+// lane 0 keeps the flushed total, so the CTA reduction still sees every unit once.
+__device__ __forceinline__ void flush_graph(unsigned long long& acc, unsigned long long& acc_total,
+                                            unsigned long long* graph_counts, uint32_t g, int lane)
+{
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) acc += __shfl_xor_sync(kFull, acc, d);
+    if (lane == 0 && g != 0xffffffffu) {
+        if (acc) atomicAdd(&graph_counts[g], acc);
+        acc_total += acc;
+    }
+    acc = 0;
+}
+
 template <int C>
 __global__ void __launch_bounds__(kThreads, 4)
 k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
         const uint32_t* __restrict__ row_indices, const uint32_t* __restrict__ blocks,
-        uint32_t num_tiles, int32_t R, int64_t n_col_blocks, int tau, uint32_t chunk,
-        CountScratch scr)
+        uint32_t num_tiles, int32_t R, int tau, uint32_t chunk, CountScratch scr,
+        const uint32_t* __restrict__ graph_rows, uint32_t num_graphs,
+        unsigned long long* __restrict__ graph_counts)
 {
     using K = Cfg<C>;
     constexpr int WPR = K::WPR, TW = K::TW, JPT = K::JPT;
@@ -282,7 +301,11 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
     const int g = lane >> 2, tg = lane & 3;  // mma fragment coordinates
 
     unsigned long long acc = 0;
-    const bool bitmap_ok = n_col_blocks <= (int64_t)kBmWords * 32;
+    // Batches (graph_counts != nullptr): the tiles of graph g are row blocks
+    // [graph_rows[g], graph_rows[g+1]); acc is flushed to graph_counts[g] whenever the
+    // row block moves to another graph, and acc_total keeps what was flushed.
+    unsigned long long acc_total = 0;
+    uint32_t g_cur = 0xffffffffu;
 
     for (;;) {
       unsigned long long c0 = 0;
@@ -336,8 +359,20 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
         }
 
         if (I != curI) {
-            A = stage_row<C>(s, indptr, indices, I, bitmap_ok, lane);
+            A = stage_row<C>(s, indptr, indices, I, lane);
             curI = I;
+            if (graph_counts) {
+                uint32_t lo = 0, hi = num_graphs;  // last g with graph_rows[g] <= I
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (graph_rows[mid] <= I) lo = mid;
+                    else hi = mid;
+                }
+                if (lo != g_cur) {
+                    flush_graph(acc, acc_total, graph_counts, g_cur, lane);
+                    g_cur = lo;
+                }
+            }
         }
         if (lane <= JPT) {
             const int64_t J = (int64_t)JL * JPT + lane;
@@ -484,6 +519,11 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
       }
     }
 
+    if (graph_counts) {
+        flush_graph(acc, acc_total, graph_counts, g_cur, lane);
+        acc = acc_total;
+    }
+
     // ---- int64 block tree + last-CTA reduction ------------------------------
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) acc += __shfl_down_sync(kFull, acc, d);
@@ -533,8 +573,8 @@ int count_grid_size(int tile_cols)
 
 int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
                  const uint32_t* row_indices, const uint32_t* blocks, uint32_t num_tiles,
-                 int32_t n_row_blocks, int64_t n_col_blocks, int tau, CountScratch scr,
-                 cudaStream_t s)
+                 int32_t n_row_blocks, int tau, CountScratch scr, cudaStream_t s,
+                 const uint32_t* graph_rows, uint32_t num_graphs, unsigned long long* graph_counts)
 {
     const int grid = count_grid_size(tile_cols);
     // About eight queue grabs per warp, between 8 and 64 consecutive tiles per grab: the
@@ -545,11 +585,12 @@ int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
     if (chunk > 64) chunk = 64;
     if (tile_cols == 128)
         k_count<128><<<grid, kThreads, 0, s>>>(indptr, indices, row_indices, blocks, num_tiles,
-                                               n_row_blocks, n_col_blocks, tau, (uint32_t)chunk,
-                                               scr);
+                                               n_row_blocks, tau, (uint32_t)chunk, scr,
+                                               graph_rows, num_graphs, graph_counts);
     else
         k_count<32><<<grid, kThreads, 0, s>>>(indptr, indices, row_indices, blocks, num_tiles,
-                                              n_row_blocks, n_col_blocks, tau, (uint32_t)chunk, scr);
+                                              n_row_blocks, tau, (uint32_t)chunk, scr, graph_rows,
+                                              num_graphs, graph_counts);
     return cudaGetLastError() == cudaSuccess ? BTC_OK : BTC_E_CUDA;
 }
 

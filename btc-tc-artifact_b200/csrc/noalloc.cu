@@ -83,7 +83,6 @@ extern "C" int btc_count_bcsr_noalloc(const btc_bcsr_device* b, int tile_cols, i
         cudaMemsetAsync(scratch + kNoAllocMaxCtas, 0, 2 * sizeof(unsigned long long), stream));
     CountScratch scr{scratch, reinterpret_cast<unsigned int*>(scratch + kNoAllocMaxCtas),
                      scratch + kNoAllocMaxCtas + 1, out, nullptr};
-    const int64_t ncb = ((int64_t)b->n + tile_cols - 1) / tile_cols;
     return launch_count(tile_cols, b->indptr, b->indices, b->row_indices, b->blocks, b->num_blocks,
-                        b->n_row_blocks, ncb, tau, scr, stream);
+                        b->n_row_blocks, tau, scr, stream);
 }

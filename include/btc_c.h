@@ -190,6 +190,46 @@ BTC_API int btc_density_hist(btc_bitbsr* g, btc_stream_t stream, uint64_t* hist)
 /* Releases the handle and every buffer it owns.  NULL is a no-op. */
 BTC_API void btc_free(btc_bitbsr* g);
 
+/* ======================================================================== */
+/* Batches: many graphs, one build, one persistent count launch               */
+/* (no counterpart in the reference, which counts one graph per process)      */
+/* ======================================================================== */
+
+typedef struct btc_batch btc_batch; /* opaque, device-resident */
+
+/* Builds the Bit-BSR of num_graphs graphs at once.  Graph g's edges are
+ * (src[i], dst[i]) for i in [edge_offsets[g], edge_offsets[g+1]) with local vertex ids in
+ * [0, num_vertices[g]); edge_offsets (num_graphs+1 entries, edge_offsets[0] = 0) and
+ * num_vertices are host arrays.  src/dst are device arrays, or host arrays with
+ * BTC_INPUT_ON_HOST.  The batch is the block-diagonal union of the graphs (graph g's
+ * vertex v is union vertex 16*R_<g + v, R_<g = row blocks of graphs 0..g-1), with one
+ * tile width for all (32, 128, or 0 for the BTC-Lite policy on the totals).
+ * Synchronises `stream` once. */
+BTC_API int btc_batch_build(const int32_t* src, const int32_t* dst, const int64_t* edge_offsets,
+                            const int32_t* num_vertices, int32_t num_graphs, int tile_cols,
+                            uint32_t flags, btc_stream_t stream, btc_batch** out);
+
+/* Rebuilds into an existing batch, reusing its device buffers when large enough. */
+BTC_API int btc_batch_rebuild(btc_batch* b, const int32_t* src, const int32_t* dst,
+                              const int64_t* edge_offsets, const int32_t* num_vertices,
+                              int32_t num_graphs, int tile_cols, uint32_t flags,
+                              btc_stream_t stream);
+
+/* Counts every graph of the batch in one launch.  d_counts (device, num_graphs uint64,
+ * nullable: the batch's own buffer) receives graph g's count at index g; with h_counts
+ * (host, nullable) the counts are also copied out and the call waits for them. */
+BTC_API int btc_batch_count(btc_batch* b, int tau, btc_stream_t stream,
+                            unsigned long long* d_counts, unsigned long long* h_counts);
+
+/* The union graph's Bit-BSR (reference layout) and sizes. */
+BTC_API int btc_batch_info(const btc_batch* b, btc_bitbsr_view* v);
+
+/* First row block of each graph in the union (num_graphs+1 host entries). */
+BTC_API int btc_batch_row_offsets(const btc_batch* b, uint32_t* row_offsets);
+
+/* Releases the batch.  NULL is a no-op. */
+BTC_API void btc_batch_free(btc_batch* b);
+
 /* Default tau for a tile width (the value BTC_TAU_DEFAULT resolves to). */
 BTC_API int btc_default_tau(int tile_cols);
 
