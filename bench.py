@@ -294,6 +294,123 @@ def run_batch(args, rank, world):
         print(json.dumps(line), flush=True)
 
 
+def raw_rmat(scale: int, edge_factor: int, seed: int):
+    """R-MAT draws without dedup (the builder removes duplicates and self-loops)."""
+    gr = np.random.default_rng(seed)
+    m = edge_factor << scale
+    u = np.zeros(m, np.int64)
+    v = np.zeros(m, np.int64)
+    for _ in range(scale):
+        r = gr.random(m, dtype=np.float32)
+        u = (u << 1) | (r >= 0.76)
+        v = (v << 1) | (((r >= 0.57) & (r < 0.76)) | (r >= 0.95))
+    return u.astype(np.int32), v.astype(np.int32), 1 << scale
+
+
+def serve_once(Server, cfg, pool, large, lam, n_req, seed, want, large_frac=0.05):
+    """Poisson arrivals at rate lam (a large_frac share of large requests, the rest from
+    the pool) into one server, after a warm-up that grows every slot's buffers; returns
+    throughput and latency percentiles on the server's clock."""
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / lam, n_req)
+    picks = [("L", int(rng.integers(len(large)))) if rng.random() < large_frac
+             else ("S", int(rng.integers(len(pool)))) for _ in range(n_req)]
+    srv = Server(**cfg)
+    # warm-up (not measured): every large request, then the pool twice, on every slot
+    warm = 0
+    for _ in range(max(1, cfg.get("slots", 2))):
+        for s_, d_, n_ in (large if large_frac > 0 else []) + pool + pool:
+            srv.submit(s_, d_, n_, borrow=True)
+            warm += 1
+    got = 0
+    while got < warm:
+        got += len(srv.poll(wait_ms=100))
+    ids = {}
+    results = []
+    done_flag = threading.Event()
+
+    def collector():
+        while not done_flag.is_set() or len(results) < n_req:
+            results.extend(srv.poll(wait_ms=20))
+            if len(results) >= n_req:
+                break
+
+    th = threading.Thread(target=collector, daemon=True)
+    th.start()
+    t_next = time.perf_counter()
+    for gap, (kind, k) in zip(gaps, picks):
+        t_next += gap
+        dt = t_next - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        s_, d_, n_ = (large if kind == "L" else pool)[k]
+        ids[srv.submit(s_, d_, n_, borrow=True)] = (kind, k)
+    done_flag.set()
+    th.join(timeout=600)
+    st = srv.stats()
+    srv.close()
+    assert len(results) == n_req, (len(results), n_req)
+    lat = np.array([r["done_s"] - r["submit_s"] for r in results])
+    for r in results:
+        assert r["status"] == 0 and r["count"] == want[ids[r["id"]]], r
+    span = max(r["done_s"] for r in results) - min(r["submit_s"] for r in results)
+    edges = sum(r["m"] for r in results)
+    return {"lambda": lam, "requests": n_req, "graphs_per_s": n_req / span,
+            "edges_per_s": edges / span, "p50_ms": float(np.percentile(lat, 50) * 1e3),
+            "p99_ms": float(np.percentile(lat, 99) * 1e3), "batches": int(st["batches"]),
+            "peak_device_gb": st["peak_device_bytes"] / 1e9}
+
+
+def run_serve(args, rank, world):
+    """Served stream: Poisson arrivals of mixed requests into the continuous-batching
+    server, against the plain per-request server, over a sweep of arrival rates."""
+    import torch
+    from btc_b200 import BitBSR, Server, graphs as G
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    def pinned(g):  # requests arrive in pinned host buffers (the server DMAs them directly)
+        s_, d_, n_ = g
+        return (torch.from_numpy(np.ascontiguousarray(s_)).pin_memory().numpy(),
+                torch.from_numpy(np.ascontiguousarray(d_)).pin_memory().numpy(), n_)
+
+    pool = [pinned((s, d, n)) for s, d, n, _ in G.batch_mix(args.pool, 256, args.n_max, seed=13)]
+    large = [pinned(raw_rmat(20, 16, seed=21)), pinned(G.stencil7(128))]
+    want = {}
+    tile = args.tile if args.tile is not None else 32
+    for kind, lst in (("S", pool), ("L", large)):
+        for k, (s_, d_, n_) in enumerate(lst):
+            want[(kind, k)] = BitBSR(torch.from_numpy(s_).cuda(), torch.from_numpy(d_).cuda(),
+                                     n_, tile).count()
+    lams = [float(x) for x in args.rates.split(",")]
+    modes = {"batched": dict(slots=2, max_batch_graphs=4096, tile_cols=tile,
+                             hbm_budget_bytes=150 << 30),
+             "plain": dict(slots=1, max_batch_graphs=1, tile_cols=tile, hbm_budget_bytes=150 << 30)}
+    sweep = []
+    for lam in lams:
+        row = {"lambda": lam}
+        for name, cfg in modes.items():
+            row[name] = serve_once(Server, cfg, pool, large, lam, args.requests, 99, want,
+                                   args.large_frac)
+            log(name, json.dumps(row[name]))
+        sweep.append(row)
+    top = sweep[-1]
+    line = {
+        "metric": "served_graphs_per_s", "value": world * top["batched"]["graphs_per_s"],
+        "unit": "graphs/s", "n_gpus": world, "steps": len(lams), "warmup": 0,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic",
+        "config": {"workload": f"Poisson stream, {100 - 100 * args.large_frac:g}% mixed graphs "
+                               f"(n log-uniform [256, {args.n_max}]), {100 * args.large_frac:g}% "
+                               f"large (R-MAT scale 20 ef 16, 7-point stencil 128^3)",
+                   "requests_per_rate": args.requests,
+                   "rates": lams, "hbm_budget_gb": 150, "tile": f"16x{tile}"},
+        "p50_ms": top["batched"]["p50_ms"], "p99_ms": top["batched"]["p99_ms"],
+        "plain": top["plain"], "speedup_vs_plain": top["batched"]["graphs_per_s"] /
+        top["plain"]["graphs_per_s"], "sweep": sweep,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -306,6 +423,10 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=8.0)
     ap.add_argument("--graphs", type=int, default=4096, help="batch workload: graphs")
     ap.add_argument("--n-max", type=int, default=65536, help="batch workload: largest n")
+    ap.add_argument("--pool", type=int, default=512, help="serve workload: distinct small graphs")
+    ap.add_argument("--requests", type=int, default=2000, help="serve workload: requests per rate")
+    ap.add_argument("--rates", default="50,200,1000,5000", help="serve workload: arrivals/s")
+    ap.add_argument("--large-frac", type=float, default=0.05, help="serve workload: large share")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -318,6 +439,9 @@ def main():
         return
     if args.workload == "batch":
         run_batch(args, rank, world)
+        return
+    if args.workload == "serve":
+        run_serve(args, rank, world)
         return
 
     import torch

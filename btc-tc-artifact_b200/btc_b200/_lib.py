@@ -51,6 +51,12 @@ EXPORTS = [
     "btc_batch_info",
     "btc_batch_row_offsets",
     "btc_batch_free",
+    "btc_server_default_config",
+    "btc_server_create",
+    "btc_server_submit",
+    "btc_server_poll",
+    "btc_server_stats_get",
+    "btc_server_destroy",
 ]
 
 
@@ -79,6 +85,27 @@ class BtcBitbsrView(C.Structure):
         ("input_edges", C.c_int64),
         ("device_bytes", C.c_size_t),
     ]
+
+
+class BtcServerConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_batch_graphs", C.c_int32),
+                ("slots", C.c_int32), ("max_batch_edges", C.c_int64), ("tile_cols", C.c_int),
+                ("tau", C.c_int), ("solo_edges", C.c_int64)]
+
+
+class BtcServerResult(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("count", C.c_ulonglong), ("status", C.c_int32),
+                ("n", C.c_int32), ("m", C.c_int64), ("submit_s", C.c_double),
+                ("done_s", C.c_double)]
+
+
+class BtcServerStats(C.Structure):
+    _fields_ = [("batches", C.c_uint64), ("graphs", C.c_uint64), ("edges", C.c_uint64),
+                ("rejected", C.c_uint64), ("queued", C.c_uint64),
+                ("peak_device_bytes", C.c_uint64), ("now_s", C.c_double)]
+
+
+BTC_SUBMIT_BORROW = 0x1
 
 
 class BtcError(RuntimeError):
@@ -132,8 +159,17 @@ def lib():
         L.btc_batch_row_offsets.argtypes = [vp, vp]
         L.btc_batch_free.argtypes = [vp]
         L.btc_batch_free.restype = None
+        L.btc_server_default_config.argtypes = [P(BtcServerConfig)]
+        L.btc_server_default_config.restype = None
+        L.btc_server_create.argtypes = [P(BtcServerConfig), P(vp)]
+        L.btc_server_submit.argtypes = [vp, vp, vp, i64, i32, u32, P(C.c_uint64)]
+        L.btc_server_poll.argtypes = [vp, P(BtcServerResult), C.c_int, P(C.c_int), C.c_int]
+        L.btc_server_stats_get.argtypes = [vp, P(BtcServerStats)]
+        L.btc_server_destroy.argtypes = [vp]
+        L.btc_server_destroy.restype = None
         for name in EXPORTS:
-            if name not in ("btc_bcsr_free", "btc_free", "btc_strerror", "btc_batch_free"):
+            if name not in ("btc_bcsr_free", "btc_free", "btc_strerror", "btc_batch_free",
+                            "btc_server_default_config", "btc_server_destroy"):
                 getattr(L, name).restype = C.c_int
         _L = L
     return _L

@@ -31,7 +31,7 @@ __all__ = [
     "convert_coo_to_bcsr_16x128_gpu", "convert_coo_to_bcsr_16x32_gpu",
     "count_triangles_16x128_adaptive", "count_triangles_16x32_adaptive",
     "preprocess_for_triangle_counting", "lite_select_tile_cols", "BitBSR", "default_tau",
-    "Batch",
+    "Batch", "Server",
 ]
 
 
@@ -413,5 +413,68 @@ class Batch:
     def __del__(self):
         try:
             self.free()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching count server (btc_server_*).  slots=1, max_batch_graphs=1 is
+    the plain one-request-at-a-time path."""
+
+    def __init__(self, hbm_budget_bytes: int | None = None, max_batch_graphs: int | None = None,
+                 slots: int | None = None, max_batch_edges: int | None = None,
+                 tile_cols: int | None = None, tau: int | None = None,
+                 solo_edges: int | None = None):
+        cfg = _lib.BtcServerConfig()
+        lib().btc_server_default_config(C.byref(cfg))
+        for k, v in dict(hbm_budget_bytes=hbm_budget_bytes, max_batch_graphs=max_batch_graphs,
+                         slots=slots, max_batch_edges=max_batch_edges, tile_cols=tile_cols,
+                         tau=tau, solo_edges=solo_edges).items():
+            if v is not None:
+                setattr(cfg, k, v)
+        self._h = C.c_void_p(None)
+        self._keep = {}
+        check(lib().btc_server_create(C.byref(cfg), C.byref(self._h)), "btc_server_create")
+
+    def submit(self, src, dst, n: int, borrow: bool = False) -> int:
+        """Queue one request (numpy int32 arrays).  borrow=True reads the arrays in place
+        (they are kept referenced here until the result is polled)."""
+        s = np.ascontiguousarray(src, np.int32)
+        d = np.ascontiguousarray(dst, np.int32)
+        rid = C.c_uint64(0)
+        check(lib().btc_server_submit(self._h, s.ctypes.data, d.ctypes.data, len(s), int(n),
+                                      _lib.BTC_SUBMIT_BORROW if borrow else 0, C.byref(rid)),
+              "btc_server_submit")
+        if borrow:
+            self._keep[int(rid.value)] = (s, d)
+        return int(rid.value)
+
+    def poll(self, max_results: int = 4096, wait_ms: int = 0) -> list:
+        buf = (_lib.BtcServerResult * max_results)()
+        k = C.c_int(0)
+        check(lib().btc_server_poll(self._h, buf, max_results, C.byref(k), int(wait_ms)),
+              "btc_server_poll")
+        out = []
+        for i in range(k.value):
+            r = buf[i]
+            self._keep.pop(int(r.id), None)
+            out.append(dict(id=int(r.id), count=int(r.count), status=int(r.status), n=int(r.n),
+                            m=int(r.m), submit_s=float(r.submit_s), done_s=float(r.done_s)))
+        return out
+
+    def stats(self) -> dict:
+        st = _lib.BtcServerStats()
+        check(lib().btc_server_stats_get(self._h, C.byref(st)), "btc_server_stats_get")
+        return {k: getattr(st, k) for k, _ in st._fields_}
+
+    def close(self) -> None:
+        if self._h:
+            lib().btc_server_destroy(self._h)
+            self._h = C.c_void_p(None)
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
         except Exception:
             pass

@@ -369,6 +369,14 @@ static int batch_build_into(btc_batch* b, const int32_t* src, const int32_t* dst
     return cudaGetLastError() == cudaSuccess ? BTC_OK : BTC_E_CUDA;
 }
 
+namespace btc200 {
+size_t batch_device_bytes(const btc_batch* b)
+{
+    return b->g.device_bytes() + b->segs.bytes + b->e_off.bytes + b->bm_off.bytes +
+           b->row_off.bytes + b->counts.bytes;
+}
+}  // namespace btc200
+
 extern "C" {
 
 int btc_batch_build(const int32_t* src, const int32_t* dst, const int64_t* edge_offsets,

@@ -323,7 +323,9 @@ int btc_bitbsr_info(const btc_bitbsr* gc, btc_bitbsr_view* v)
     if (!gc || !v) return BTC_E_INVAL;
     btc_bitbsr* g = const_cast<btc_bitbsr*>(gc);
     if (!g->edges_known) {
-        // unique lower edges = bits set in the tiles (duplicates OR the same bit)
+        // unique lower edges = bits set in the tiles (duplicates OR the same bit); the
+        // build may have run on any stream, so wait for the device first
+        BTC_CUDA_TRY(cudaDeviceSynchronize());
         unsigned long long u = 0;
         unsigned long long* d = g->meta.as<unsigned long long>() + kMetaUniq;
         BTC_TRY(launch_popcount_sum(g->tile_cols, g->blocks.as<uint32_t>(), g->num_tiles, d, nullptr));

@@ -230,6 +230,67 @@ BTC_API int btc_batch_row_offsets(const btc_batch* b, uint32_t* row_offsets);
 /* Releases the batch.  NULL is a no-op. */
 BTC_API void btc_batch_free(btc_batch* b);
 
+/* ======================================================================== */
+/* Serving: continuous batching over the batched path                        */
+/* (no counterpart in the reference)                                          */
+/* ======================================================================== */
+
+typedef struct btc_server btc_server; /* opaque; owns one engine thread */
+
+typedef struct btc_server_config {
+    uint64_t hbm_budget_bytes; /* device memory all batch slots together may hold */
+    int32_t max_batch_graphs;  /* requests per batch (1: no batching) */
+    int32_t slots;             /* batches in flight at once (1..8; 2 overlaps them) */
+    int64_t max_batch_edges;   /* input edges per batch */
+    int tile_cols;             /* 32, 128, or 0 for the BTC-Lite policy per batch */
+    int tau;                   /* dense/sparse switch, BTC_TAU_DEFAULT */
+    int64_t solo_edges;        /* requests with at least this many edges run alone,
+                                  degree-ordered, with the BTC-Lite tile width */
+} btc_server_config;
+
+typedef struct btc_server_result {
+    uint64_t id;              /* from btc_server_submit */
+    unsigned long long count; /* triangles (0 unless status == BTC_OK) */
+    int32_t status;           /* BTC_OK, or BTC_E_NOMEM if the request alone exceeds
+                                 the budget, or the failing call's status */
+    int32_t n;                /* the request's vertex count */
+    int64_t m;                /* the request's edge count */
+    double submit_s;          /* server steady clock, seconds */
+    double done_s;            /* when the result was published */
+} btc_server_result;
+
+typedef struct btc_server_stats {
+    uint64_t batches, graphs, edges, rejected, queued, peak_device_bytes;
+    double now_s;
+} btc_server_stats;
+
+/* Fills the defaults: 150 GB budget, 4096 graphs and 256M edges per batch, 2 slots,
+ * 16x32 tiles, default tau, requests of 2^20 edges or more run alone. */
+BTC_API void btc_server_default_config(btc_server_config* cfg);
+
+/* Starts a server on the current device.  A batch slot admits queued requests in
+ * arrival order while the batch stays within the caps and all slots stay within the
+ * budget; requests that arrive while batches are on the GPU join the next batch. */
+BTC_API int btc_server_create(const btc_server_config* cfg, btc_server** out);
+
+/* Queues a request (host edge arrays; local ids in [0, n)).  Returns at once;
+ * *id_out identifies the result.  The edges are copied on submit, or, with
+ * BTC_SUBMIT_BORROW, read in place when the request's batch is staged: the caller then
+ * keeps src/dst unchanged until the request's result has been polled. */
+#define BTC_SUBMIT_BORROW 0x1u
+BTC_API int btc_server_submit(btc_server* s, const int32_t* src, const int32_t* dst, int64_t m,
+                              int32_t n, uint32_t flags, uint64_t* id_out);
+
+/* Moves up to max_results finished results to out (*n_out of them), waiting up to
+ * wait_ms for the first one. */
+BTC_API int btc_server_poll(btc_server* s, btc_server_result* out, int max_results, int* n_out,
+                            int wait_ms);
+
+BTC_API int btc_server_stats_get(btc_server* s, btc_server_stats* st);
+
+/* Finishes every queued request, then stops the engine and frees the server. */
+BTC_API void btc_server_destroy(btc_server* s);
+
 /* Default tau for a tile width (the value BTC_TAU_DEFAULT resolves to). */
 BTC_API int btc_default_tau(int tile_cols);
 

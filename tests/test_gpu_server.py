@@ -1,0 +1,83 @@
+"""GPU tests of the continuous-batching server (btc_server_*): every request's count is
+the same alone (plain path, and the single-graph BitBSR) and in the mix, whatever
+batch it lands in and however its arrival overlaps others on the device.  Counts are
+integers, so the tolerance is zero."""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+from btc_b200 import BitBSR, Server, graphs as G, _lib  # noqa: E402
+
+
+def _pool():
+    gs = [(s, d, n) for s, d, n, _ in G.batch_mix(40, 256, 4096, seed=5)]
+    gs.append(G.stencil7(24))
+    gs.append(G.stencil27(20))
+    return gs
+
+
+def _alone(gs):
+    return [BitBSR(torch.from_numpy(s).cuda(), torch.from_numpy(d).cuda(), n, 32).count()
+            for s, d, n in gs]
+
+
+def _run(server, gs, order, gap_s=0.0, borrow=False):
+    ids = {}
+    for k in order:
+        s, d, n = gs[k]
+        ids[server.submit(s, d, n, borrow=borrow)] = k
+        if gap_s:
+            time.sleep(gap_s)
+    got = {}
+    deadline = time.time() + 120
+    while len(got) < len(ids) and time.time() < deadline:
+        for r in server.poll(wait_ms=100):
+            assert r["status"] == 0
+            assert r["done_s"] >= r["submit_s"]
+            got[r["id"]] = r["count"]
+    assert len(got) == len(ids)
+    return [(ids[i], c) for i, c in got.items()]
+
+
+@pytest.mark.parametrize("slots,max_graphs,borrow", [(2, 4096, False), (2, 7, True), (1, 1, False),
+                                                     (3, 16, True)])
+def test_counts_same_alone_and_in_the_mix(slots, max_graphs, borrow):
+    gs = _pool()
+    want = _alone(gs)
+    rng = np.random.default_rng(slots * 100 + max_graphs)
+    order = list(rng.permutation(len(gs))) * 3
+    srv = Server(slots=slots, max_batch_graphs=max_graphs)
+    for k, c in _run(srv, gs, order, gap_s=0.0005, borrow=borrow):
+        assert c == want[k]
+    st = srv.stats()
+    assert st["graphs"] == len(order) and st["rejected"] == 0
+    if max_graphs > 1:
+        assert st["batches"] < len(order)  # requests were batched
+    srv.close()
+
+
+def test_budget_rejects_a_request_too_large_alone():
+    srv = Server(hbm_budget_bytes=1 << 20)  # 1 MiB: nothing but the smallest fits
+    s, d, n = G.stencil27(32)
+    rid = srv.submit(s, d, n)
+    res = []
+    while not res:
+        res = srv.poll(wait_ms=200)
+    assert res[0]["id"] == rid and res[0]["status"] == _lib.BTC_E_NOMEM
+    assert srv.stats()["rejected"] == 1
+    srv.close()
+
+
+def test_close_drains_queue():
+    gs = _pool()
+    srv = Server()
+    for s, d, n in gs:
+        srv.submit(s, d, n)
+    srv.close()  # returns after every queued request ran
