@@ -141,14 +141,19 @@ class ClockSampler:
 
 
 def launches_per_step(n: int, tile_cols: int, orient_degree: bool, m: int) -> int:
-    """Kernels the engine launches per build + count (see csrc/capi.cu build_into)."""
+    """Kernels the engine launches per build + count (csrc/capi.cu build_into): the
+    bitmap builder (mark, chunk count, scan, emit, last indptr, fill) when the cell
+    bitmap is small enough, else the radix builder; plus the degree relabel and count."""
     R = (n + 15) // 16
     ncb = (n + tile_cols - 1) // tile_cols
-    t_bits = max(R - 1, 0).bit_length() + max(ncb - 1, 0).bit_length()
-    passes = -(-t_bits // 8)
-    k = 1 + 3 * passes + 2 + 1 + 1  # keys, sort, segment (2), fill, indptr
+    bm_bytes = 4 * R * ((ncb + 31) // 32)
+    if bm_bytes <= (4 << 30) and bm_bytes <= 32 * m + (64 << 20):
+        k = 6
+    else:
+        t_bits = max(R - 1, 0).bit_length() + max(ncb - 1, 0).bit_length()
+        k = 1 + 3 * (-(-t_bits // 8)) + 2 + 1 + 1  # keys, sort, segment (2), fill, indptr
     if orient_degree:
-        db = max(1, (2 * m).bit_length())
+        db = min(32, max(1, (2 * m).bit_length()))
         k += 1 + 1 + 1 + 3 * (-(-db // 8)) + 1  # degree, rank keys, set count, sort, scatter
     return k + 1  # count
 
@@ -612,7 +617,8 @@ def main():
                                         "sample": f"full graph, median of {reps_cpu} counts"}
             if O.ref_gpu_available() and not args.no_ref_gpu:
                 rr, cc = rp_to_coo(rp, col)
-                ref = O.ref_gpu_run(rr, cc, n, tile, warmup=3, repeat=20)
+                big = B > 2_000_000
+                ref = O.ref_gpu_run(rr, cc, n, tile, warmup=1 if big else 3, repeat=3 if big else 20)
                 assert ref["count"] == expected, (ref["count"], expected)
                 kms = statistics.median(ref["kernel_ms"])
                 line["reference_gpu"] = {
