@@ -343,3 +343,48 @@ int launch_bitmap_count(const uint32_t* bitmap, uint64_t W, uint32_t* chunk_coun
     return cudaGetLastError() == cudaSuccess ? BTC_OK : BTC_E_CUDA;
 }
 }  // namespace btc200
+
+namespace btc200 {
+namespace bm {
+template <int WPR>
+__global__ void k_rowmask(const uint32_t* __restrict__ blocks, uint32_t num_tiles,
+                          uint32_t* __restrict__ rowmask)
+{
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < num_tiles;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t* b = blocks + t * (16 * WPR);
+        uint32_t m = 0;
+        if constexpr (WPR == 4) {
+#pragma unroll
+            for (int r = 0; r < 16; ++r) {
+                const uint4 v = reinterpret_cast<const uint4*>(b)[r];
+                m |= ((v.x | v.y | v.z | v.w) != 0u) ? (1u << r) : 0u;
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const uint4 v = reinterpret_cast<const uint4*>(b)[q];
+                m |= (v.x != 0u ? 1u : 0u) << (4 * q);
+                m |= (v.y != 0u ? 1u : 0u) << (4 * q + 1);
+                m |= (v.z != 0u ? 1u : 0u) << (4 * q + 2);
+                m |= (v.w != 0u ? 1u : 0u) << (4 * q + 3);
+            }
+        }
+        rowmask[t] = m;
+    }
+}
+}  // namespace bm
+
+int launch_rowmask(int tile_cols, const uint32_t* blocks, uint32_t num_tiles, uint32_t* rowmask,
+                   cudaStream_t s)
+{
+    if (num_tiles) {
+        const int grid = grid_for((int64_t)num_tiles, 256);
+        if (tile_cols == 128)
+            bm::k_rowmask<4><<<grid, 256, 0, s>>>(blocks, num_tiles, rowmask);
+        else
+            bm::k_rowmask<1><<<grid, 256, 0, s>>>(blocks, num_tiles, rowmask);
+    }
+    return cudaGetLastError() == cudaSuccess ? BTC_OK : BTC_E_CUDA;
+}
+}  // namespace btc200

@@ -20,6 +20,16 @@
 //    the slices that have bits (32 per round, one per lane) in row block I's structure.
 //    This replaces the reference's serial two-pointer merge, repeated per slice by all
 //    32 lanes, with one parallel search per tile.
+//  * Optional per-tile row-occupancy masks (bit r: tile row r has a bit) drop matches
+//    whose I tile has no occupied row among S's rows of the slice, or whose J_out tile
+//    has none among its columns, and skip units with an empty row on either side before
+//    any tile row is read.  On power-law graphs most matches are such empty pairs.
+//  * When the Bit-BSR came from the cell-bitmap builder, each slice is searched in the
+//    cheaper direction: J_out's list elements looked up in row block I's structure, or
+//    the elements of I's list that fall inside J_out's column span looked up in J_out's
+//    (row block, column block) cell-bitmap row, ranked with the builder's per-word tile
+//    prefix.  On degree-ordered power-law graphs J_out is usually a hub block whose span
+//    holds few of I's elements.
 //  * Sparse path: matches are appended in slice order (slice j owns entries
 //    [mc[j], mc[j+1])).  Each set bit (r, c) of S then adds popc(L[I,K][r] & L[J_out,K][c])
 //    over its slice's matches, with the lanes spread over bits (many bits, few matches:
@@ -62,6 +72,12 @@ struct __align__(16) WarpSmem {
     uint32_t mc[Cfg<C>::JPT + 1];    // match-list start of each slice
     uint32_t mpa[kMCap];             // matched tile of row block I
     uint32_t mpb[kMCap];             // matched tile of row block J_out
+    uint16_t mra[kMCap];             // occupied rows of the matched I tile
+    uint16_t mrb[kMCap];             // occupied rows of the matched J_out tile
+    uint32_t sstart[Cfg<C>::JPT];    // search list start of slice j (tile index)
+    uint8_t sdir[Cfg<C>::JPT];       // 0: J_out's list searched in I; 1: I's list in J_out
+    uint16_t rmask[Cfg<C>::JPT];     // rows of S with bits in slice j
+    uint16_t cmask[Cfg<C>::JPT];     // columns (rows of J_out tiles) with bits in slice j
     uint16_t bits[kBCap];            // (row << 8) | column of the sample tile's set bits
 };
 
@@ -69,6 +85,7 @@ struct __align__(16) WarpSmem {
 struct ARow {
     uint32_t start;  // indptr[I]
     uint32_t len;    // number of tiles in row block I
+    uint32_t last;   // last column block of row block I
     uint32_t base;   // bitmap mode: first column block of the bitmap (multiple of 32)
     uint32_t words;  // bitmap mode: bitmap words in use
     int mode;        // 0: sorted list in shared memory, 1: bitmap, 2: sorted list in HBM
@@ -103,6 +120,17 @@ __device__ __forceinline__ uint32_t slice_of(const uint32_t* S, int r, int j)
     return (S[r * WPR + ((16 * j) >> 5)] >> ((16 * j) & 31)) & 0xFFFFu;
 }
 
+// Bits 0, 2, 4, ... 30 of x, packed into bits 0..15.
+__device__ __forceinline__ uint32_t compress_even(uint32_t x)
+{
+    x &= 0x55555555u;
+    x = (x | (x >> 1)) & 0x33333333u;
+    x = (x | (x >> 2)) & 0x0F0F0F0Fu;
+    x = (x | (x >> 4)) & 0x00FF00FFu;
+    x = (x | (x >> 8)) & 0x0000FFFFu;
+    return x;
+}
+
 // Stages row block I's column-block list for lookups.  Called with the warp converged.
 // The bitmap spans the row block's own column-block range, so it is used whenever
 // that range is at most kBmWords * 32 column blocks wide.
@@ -115,7 +143,8 @@ __device__ __forceinline__ ARow stage_row(WarpSmem<C>& s, const uint32_t* __rest
     A.start = indptr[I];
     A.len = indptr[I + 1] - A.start;  // >= 1: a tile of row block I is being counted
     A.base = indices[A.start] & ~31u;
-    A.words = ((indices[A.start + A.len - 1] - A.base) >> 5) + 1;
+    A.last = indices[A.start + A.len - 1];
+    A.words = ((A.last - A.base) >> 5) + 1;
     __syncwarp();  // earlier readers of s.a / s.apre are done
     if (A.words <= (uint32_t)kBmWords) {
         A.mode = 1;
@@ -183,6 +212,21 @@ __device__ __forceinline__ bool a_lookup(const WarpSmem<C>& s, const ARow& A,
     return pos < A.len && indices[A.start + pos] == b;
 }
 
+// Number of elements of row block I's list below column block x.
+template <int C>
+__device__ __forceinline__ uint32_t a_rank(const WarpSmem<C>& s, const ARow& A,
+                                           const uint32_t* __restrict__ indices, uint32_t x)
+{
+    if (A.mode == 1) {
+        if (x <= A.base) return 0;
+        const uint32_t w = (x - A.base) >> 5;
+        if (w >= A.words) return A.len;
+        return s.apre[w] + __popc(s.a.bm[w] & ((1u << ((x - A.base) & 31u)) - 1u));
+    }
+    if (A.mode == 0) return lower_bound_u32(s.a.list, A.len, x);
+    return lower_bound_u32(indices + A.start, A.len, x);
+}
+
 // One bit pass: every set bit (r, col) of the sample tile, one per lane, adds
 // popc(L[I,K][r] & L[J_out,K][col % 16]) over the buffered matches K of its slice
 // j = col / 16, i.e. match-list entries [mc[j], mc[j+1]) clipped to [lo, hi).
@@ -229,6 +273,7 @@ __device__ __forceinline__ unsigned long long bit_pass(WarpSmem<C>& s, uint32_t 
                 const uint32_t* Ar = blocks + r * WPR;
                 const uint32_t* Br = blocks + c * WPR;
                 for (uint32_t k = k0 + lane; k < k1; k += kWarp) {
+                    if (!((s.mra[k - lo] >> r) & (s.mrb[k - lo] >> c) & 1u)) continue;
                     const size_t pa = s.mpa[k - lo], pb = s.mpb[k - lo];
                     if constexpr (C == 128) {
                         const uint4 a = *reinterpret_cast<const uint4*>(Ar + pa * TW);
@@ -250,6 +295,7 @@ __device__ __forceinline__ unsigned long long bit_pass(WarpSmem<C>& s, uint32_t 
                 const uint32_t* Ar = blocks + r * WPR;
                 const uint32_t* Br = blocks + c * WPR;
                 for (uint32_t k = k0; k < k1; ++k) {
+                    if (!((s.mra[k - lo] >> r) & (s.mrb[k - lo] >> c) & 1u)) continue;
                     const size_t pa = s.mpa[k - lo], pb = s.mpb[k - lo];
                     if constexpr (C == 128) {
                         const uint4 a = *reinterpret_cast<const uint4*>(Ar + pa * TW);
@@ -287,7 +333,8 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
         const uint32_t* __restrict__ row_indices, const uint32_t* __restrict__ blocks,
         uint32_t num_tiles, int32_t R, int tau, uint32_t chunk, CountScratch scr,
         const uint32_t* __restrict__ graph_rows, uint32_t num_graphs,
-        unsigned long long* __restrict__ graph_counts)
+        unsigned long long* __restrict__ graph_counts, const uint32_t* __restrict__ rowmask,
+        const uint32_t* __restrict__ cellbm, const uint32_t* __restrict__ cellpre, uint64_t cell_wpr)
 {
     using K = Cfg<C>;
     constexpr int WPR = K::WPR, TW = K::TW, JPT = K::JPT;
@@ -400,9 +447,64 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
                 if (lane >= d) e += y;
             }
             e -= mine;
+            // Tiles with more than one round of list elements take the heavy path: rows
+            // and columns of S that carry bits, per slice (to drop matches and units whose
+            // tile rows are empty), and the two-direction search plan.  Small tiles skip
+            // both: a single round costs less than planning it.
+            const bool heavy = upre[JPT] > (uint32_t)kWarp;
+            const uint32_t* __restrict__ rmask_g = heavy ? rowmask : nullptr;
+            uint32_t rm[JPT], cm[JPT];
+#pragma unroll
+            for (int j = 0; j < JPT; ++j) rm[j] = cm[j] = 0xFFFFu;
+            if (!heavy) {
+            } else if constexpr (C == 128) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const uint32_t sl = ((q < 2 ? w0 : w1) >> (16 * (q & 1))) & 0xFFFFu;
+                    const unsigned bl = __ballot_sync(kFull, sl != 0);
+                    rm[q] = compress_even(bl);
+                    rm[4 + q] = compress_even(bl >> 1);
+                    cm[q] = __reduce_or_sync(kFull, (lane & 1) ? 0u : sl);
+                    cm[4 + q] = __reduce_or_sync(kFull, (lane & 1) ? sl : 0u);
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const uint32_t sl = (w0 >> (16 * q)) & 0xFFFFu;
+                    rm[q] = __ballot_sync(kFull, sl != 0) & 0xFFFFu;
+                    cm[q] = __reduce_or_sync(kFull, sl);
+                }
+            }
+            // search plan: lane j < JPT picks slice j's direction and list
+            {
+                uint32_t len = 0, start = 0, dir = 0;
+                if (lane < JPT && ((active >> lane) & 1u)) {
+                    const uint32_t jb = s.jptr[lane], je = s.jptr[lane + 1];
+                    len = je - jb;
+                    start = jb;
+                    if (heavy && cellbm && je > jb) {
+                        const uint32_t r0 = a_rank<C>(s, A, indices, indices[jb]);
+                        const uint32_t r1 = a_rank<C>(s, A, indices, indices[je - 1] + 1);
+                        if (r1 - r0 < len) {
+                            len = r1 - r0;
+                            start = A.start + r0;
+                            dir = 1;
+                        }
+                    }
+                    s.sstart[lane] = start;
+                    s.sdir[lane] = (uint8_t)dir;
+                }
+#pragma unroll
+                for (int j = 0; j < JPT; ++j) upre[j + 1] = upre[j] + __shfl_sync(kFull, len, j);
+            }
             if (lane == 0) {
 #pragma unroll
                 for (int j = 0; j <= JPT; ++j) s.upre[j] = upre[j];
+#pragma unroll
+                for (int j = 0; j < JPT; ++j) {
+                    s.rmask[j] = (uint16_t)rm[j];
+                    s.cmask[j] = (uint16_t)cm[j];
+                }
             }
             __syncwarp();
             const uint32_t W = upre[JPT];
@@ -411,23 +513,40 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
             for (uint32_t ub = 0; ub < W; ub += kWarp) {
                 const uint32_t u = ub + lane;
                 bool found = false;
-                uint32_t pa = 0, pb = 0;
+                uint32_t pa = 0, pb = 0, ra = 0xFFFFu, rb = 0xFFFFu;
                 if (u < W) {
-                    uint32_t jb = s.jptr[0], us = 0;
+                    uint32_t us = 0, jsel = 0;
 #pragma unroll
                     for (int j = 1; j < JPT; ++j)
                         if (u >= upre[j]) {
-                            jb = s.jptr[j];
                             us = upre[j];
+                            jsel = j;
                         }
-                    pb = jb + (u - us);
-                    found = a_lookup<C>(s, A, indices, indices[pb], pa);
+                    const uint32_t idx = s.sstart[jsel] + (u - us);
+                    if (!s.sdir[jsel]) {
+                        pb = idx;
+                        found = a_lookup<C>(s, A, indices, indices[pb], pa);
+                    } else {
+                        pa = idx;
+                        const uint32_t a = indices[pa];
+                        const uint64_t cw = (uint64_t)(JL * JPT + jsel) * cell_wpr + (a >> 5);
+                        const uint32_t x = cellbm[cw], bit = 1u << (a & 31u);
+                        found = (x & bit) != 0u;
+                        if (found) pb = cellpre[cw] + __popc(x & (bit - 1u));
+                    }
+                    if (found && rmask_g) {
+                        ra = rmask_g[pa];
+                        rb = rmask_g[pb];
+                        found = (ra & s.rmask[jsel]) && (rb & s.cmask[jsel]);
+                    }
                 }
                 const unsigned mb = __ballot_sync(kFull, found);
                 if (found) {
                     const uint32_t k = nm - lo + __popc(mb & lt);
                     s.mpa[k] = pa;
                     s.mpb[k] = pb;
+                    s.mra[k] = (uint16_t)ra;
+                    s.mrb[k] = (uint16_t)rb;
                 }
                 if (lane <= JPT) {
                     const uint32_t lim = s.upre[lane];
@@ -574,7 +693,9 @@ int count_grid_size(int tile_cols)
 int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
                  const uint32_t* row_indices, const uint32_t* blocks, uint32_t num_tiles,
                  int32_t n_row_blocks, int tau, CountScratch scr, cudaStream_t s,
-                 const uint32_t* graph_rows, uint32_t num_graphs, unsigned long long* graph_counts)
+                 const uint32_t* graph_rows, uint32_t num_graphs, unsigned long long* graph_counts,
+                 const uint32_t* rowmask, const uint32_t* cellbm, const uint32_t* cellpre,
+                 uint64_t cell_wpr)
 {
     const int grid = count_grid_size(tile_cols);
     // About eight queue grabs per warp, between 8 and 64 consecutive tiles per grab: the
@@ -586,11 +707,13 @@ int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
     if (tile_cols == 128)
         k_count<128><<<grid, kThreads, 0, s>>>(indptr, indices, row_indices, blocks, num_tiles,
                                                n_row_blocks, tau, (uint32_t)chunk, scr,
-                                               graph_rows, num_graphs, graph_counts);
+                                               graph_rows, num_graphs, graph_counts, rowmask,
+                                               cellbm, cellpre, cell_wpr);
     else
         k_count<32><<<grid, kThreads, 0, s>>>(indptr, indices, row_indices, blocks, num_tiles,
                                               n_row_blocks, tau, (uint32_t)chunk, scr, graph_rows,
-                                              num_graphs, graph_counts);
+                                              num_graphs, graph_counts, rowmask, cellbm, cellpre,
+                                              cell_wpr);
     return cudaGetLastError() == cudaSuccess ? BTC_OK : BTC_E_CUDA;
 }
 

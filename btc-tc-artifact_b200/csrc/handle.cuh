@@ -11,7 +11,7 @@ struct btc_bitbsr {
     uint32_t num_tiles = 0;
     int64_t input_edges = 0;
     // Bit-BSR arrays (reference layout)
-    btc200::DevBuf indptr, indices, row_indices, blocks, result;
+    btc200::DevBuf indptr, indices, row_indices, blocks, result, rowmask;
     // build workspace
     btc200::DevBuf in_src, in_dst, keys0, keys1, sort_scratch, tile_base, meta, deg, rank, bitmap, prefix;
     bool used_bitmap = false;
@@ -25,7 +25,7 @@ struct btc_bitbsr {
     {
         const btc200::DevBuf* all[] = {&indptr, &indices, &row_indices, &blocks, &result, &in_src, &in_dst,
                                &keys0, &keys1, &sort_scratch, &tile_base, &meta, &deg, &rank,
-                               &bitmap, &prefix, &partials, &done};
+                               &bitmap, &prefix, &partials, &done, &rowmask};
         size_t s = 0;
         for (const btc200::DevBuf* b : all) s += b->bytes;
         return s;
@@ -34,7 +34,7 @@ struct btc_bitbsr {
     {
         btc200::DevBuf* all[] = {&indptr, &indices, &row_indices, &blocks, &result, &in_src, &in_dst,
                          &keys0, &keys1, &sort_scratch, &tile_base, &meta, &deg, &rank,
-                         &bitmap, &prefix, &partials, &done};
+                         &bitmap, &prefix, &partials, &done, &rowmask};
         for (btc200::DevBuf* b : all) b->release();
         if (h_meta) cudaFreeHost(h_meta);
         h_meta = nullptr;
