@@ -348,8 +348,17 @@ namespace btc200 {
 namespace bm {
 template <int WPR>
 __global__ void k_rowmask(const uint32_t* __restrict__ blocks, uint32_t num_tiles,
+                          const uint32_t* __restrict__ indptr, uint32_t R,
                           uint32_t* __restrict__ rowmask)
 {
+    // longest row-block list
+    uint32_t mx = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < R;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        mx = max(mx, indptr[i + 1] - indptr[i]);
+    mx = __reduce_max_sync(kFull, mx);
+    if ((threadIdx.x & 31) == 0 && mx) atomicMax(rowmask + num_tiles, mx);
+
     for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < num_tiles;
          t += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t* b = blocks + t * (16 * WPR);
@@ -375,15 +384,19 @@ __global__ void k_rowmask(const uint32_t* __restrict__ blocks, uint32_t num_tile
 }
 }  // namespace bm
 
-int launch_rowmask(int tile_cols, const uint32_t* blocks, uint32_t num_tiles, uint32_t* rowmask,
+int launch_rowmask(int tile_cols, const uint32_t* blocks, uint32_t num_tiles,
+                   const uint32_t* indptr, int32_t n_row_blocks, uint32_t* rowmask,
                    cudaStream_t s)
 {
-    if (num_tiles) {
-        const int grid = grid_for((int64_t)num_tiles, 256);
+    if (cudaMemsetAsync(rowmask + num_tiles, 0, sizeof(uint32_t), s) != cudaSuccess)
+        return BTC_E_CUDA;
+    const uint32_t R = n_row_blocks > 0 ? (uint32_t)n_row_blocks : 0u;
+    if (num_tiles || R) {
+        const int grid = grid_for((int64_t)max(num_tiles, R), 256);
         if (tile_cols == 128)
-            bm::k_rowmask<4><<<grid, 256, 0, s>>>(blocks, num_tiles, rowmask);
+            bm::k_rowmask<4><<<grid, 256, 0, s>>>(blocks, num_tiles, indptr, R, rowmask);
         else
-            bm::k_rowmask<1><<<grid, 256, 0, s>>>(blocks, num_tiles, rowmask);
+            bm::k_rowmask<1><<<grid, 256, 0, s>>>(blocks, num_tiles, indptr, R, rowmask);
     }
     return cudaGetLastError() == cudaSuccess ? BTC_OK : BTC_E_CUDA;
 }

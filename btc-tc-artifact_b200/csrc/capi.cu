@@ -216,9 +216,10 @@ static int build_into(btc_bitbsr* g, const int32_t* src, const int32_t* dst, int
         BTC_TRY(launch_indptr(g->row_indices.as<uint32_t>(), g->num_tiles, geom.n_row_blocks,
                               g->indptr.as<uint32_t>(), s));
     }
-    BTC_TRY(g->rowmask.reserve(sizeof(uint32_t) * (tiles ? tiles : 1)));
+    BTC_TRY(g->rowmask.reserve(sizeof(uint32_t) * (tiles + 1)));
     BTC_TRY(launch_rowmask(tile_cols, g->blocks.as<uint32_t>(), g->num_tiles,
-                           g->rowmask.as<uint32_t>(), s));
+                           g->indptr.as<uint32_t>(), g->n_row_blocks, g->rowmask.as<uint32_t>(),
+                           s));
     return BTC_OK;
 }
 
@@ -237,7 +238,8 @@ int count_handle(btc_bitbsr* g, int tau, cudaStream_t s, unsigned long long* d_o
                         g->rowmask.as<uint32_t>(),
                         g->used_bitmap ? g->bitmap.as<uint32_t>() : nullptr,
                         g->used_bitmap ? g->prefix.as<uint32_t>() : nullptr,
-                        bitmap_words_per_row(make_geom(g->n, g->tile_cols)));
+                        bitmap_words_per_row(make_geom(g->n, g->tile_cols)),
+                        g->rowmask.as<uint32_t>() + g->num_tiles);
 }
 
 // ===========================================================================

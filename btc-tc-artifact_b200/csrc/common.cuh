@@ -152,10 +152,13 @@ int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
                  const uint32_t* graph_rows = nullptr, uint32_t num_graphs = 0,
                  unsigned long long* graph_counts = nullptr, const uint32_t* rowmask = nullptr,
                  const uint32_t* cellbm = nullptr, const uint32_t* cellpre = nullptr,
-                 uint64_t cell_wpr = 0);
+                 uint64_t cell_wpr = 0, const uint32_t* row_max = nullptr);
 
-// rowmask[t] bit r = tile t's row r has a bit (built after the tiles are filled).
-int launch_rowmask(int tile_cols, const uint32_t* blocks, uint32_t num_tiles, uint32_t* rowmask,
+// rowmask[t] bit r = tile t's row r has a bit (built after the tiles are filled), and
+// rowmask[num_tiles] = the most tiles in one row block (indptr's largest step), which
+// picks the count kernel's schedule.  rowmask holds num_tiles + 1 words.
+int launch_rowmask(int tile_cols, const uint32_t* blocks, uint32_t num_tiles,
+                   const uint32_t* indptr, int32_t n_row_blocks, uint32_t* rowmask,
                    cudaStream_t s);
 
 // Queue/completion words of the count kernel: done (u32) at byte 0, work (u64) at 8.

@@ -135,13 +135,12 @@ __device__ __forceinline__ uint32_t compress_even(uint32_t x)
 // The bitmap spans the row block's own column-block range, so it is used whenever
 // that range is at most kBmWords * 32 column blocks wide.
 template <int C>
-__device__ __forceinline__ ARow stage_row(WarpSmem<C>& s, const uint32_t* __restrict__ indptr,
-                                          const uint32_t* __restrict__ indices, uint32_t I,
-                                          int lane)
+__device__ __forceinline__ ARow stage_row(WarpSmem<C>& s, const uint32_t* __restrict__ indices,
+                                          uint32_t start, uint32_t len, int lane)
 {
     ARow A;
-    A.start = indptr[I];
-    A.len = indptr[I + 1] - A.start;  // >= 1: a tile of row block I is being counted
+    A.start = start;
+    A.len = len;  // >= 1: a tile of row block I is being counted
     A.base = indices[A.start] & ~31u;
     A.last = indices[A.start + A.len - 1];
     A.words = ((A.last - A.base) >> 5) + 1;
@@ -230,7 +229,7 @@ __device__ __forceinline__ uint32_t a_rank(const WarpSmem<C>& s, const ARow& A,
 // One bit pass: every set bit (r, col) of the sample tile, one per lane, adds
 // popc(L[I,K][r] & L[J_out,K][col % 16]) over the buffered matches K of its slice
 // j = col / 16, i.e. match-list entries [mc[j], mc[j+1]) clipped to [lo, hi).
-template <int C>
+template <int C, bool kHeavy>
 __device__ __forceinline__ unsigned long long bit_pass(WarpSmem<C>& s, uint32_t w0, uint32_t w1,
                                                        uint32_t e, uint32_t nnz, uint32_t lo,
                                                        uint32_t hi,
@@ -272,8 +271,9 @@ __device__ __forceinline__ unsigned long long bit_pass(WarpSmem<C>& s, uint32_t 
                 const uint32_t k0 = max(s.mc[j], lo), k1 = min(s.mc[j + 1], hi);
                 const uint32_t* Ar = blocks + r * WPR;
                 const uint32_t* Br = blocks + c * WPR;
+#pragma unroll 2
                 for (uint32_t k = k0 + lane; k < k1; k += kWarp) {
-                    if (!((s.mra[k - lo] >> r) & (s.mrb[k - lo] >> c) & 1u)) continue;
+                    if (kHeavy && !((s.mra[k - lo] >> r) & (s.mrb[k - lo] >> c) & 1u)) continue;
                     const size_t pa = s.mpa[k - lo], pb = s.mpb[k - lo];
                     if constexpr (C == 128) {
                         const uint4 a = *reinterpret_cast<const uint4*>(Ar + pa * TW);
@@ -294,8 +294,9 @@ __device__ __forceinline__ unsigned long long bit_pass(WarpSmem<C>& s, uint32_t 
                 const uint32_t k0 = max(s.mc[j], lo), k1 = min(s.mc[j + 1], hi);
                 const uint32_t* Ar = blocks + r * WPR;
                 const uint32_t* Br = blocks + c * WPR;
+#pragma unroll 2
                 for (uint32_t k = k0; k < k1; ++k) {
-                    if (!((s.mra[k - lo] >> r) & (s.mrb[k - lo] >> c) & 1u)) continue;
+                    if (kHeavy && !((s.mra[k - lo] >> r) & (s.mrb[k - lo] >> c) & 1u)) continue;
                     const size_t pa = s.mpa[k - lo], pb = s.mpb[k - lo];
                     if constexpr (C == 128) {
                         const uint4 a = *reinterpret_cast<const uint4*>(Ar + pa * TW);
@@ -327,14 +328,15 @@ __device__ __forceinline__ void flush_graph(unsigned long long& acc, unsigned lo
     acc = 0;
 }
 
-template <int C>
+template <int C, bool kHeavy>
 __global__ void __launch_bounds__(kThreads, 4)
 k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
         const uint32_t* __restrict__ row_indices, const uint32_t* __restrict__ blocks,
         uint32_t num_tiles, int32_t R, int tau, uint32_t chunk, CountScratch scr,
         const uint32_t* __restrict__ graph_rows, uint32_t num_graphs,
         unsigned long long* __restrict__ graph_counts, const uint32_t* __restrict__ rowmask,
-        const uint32_t* __restrict__ cellbm, const uint32_t* __restrict__ cellpre, uint64_t cell_wpr)
+        const uint32_t* __restrict__ cellbm, const uint32_t* __restrict__ cellpre, uint64_t cell_wpr,
+        uint32_t chunk_skewed, const uint32_t* __restrict__ row_max)
 {
     using K = Cfg<C>;
     constexpr int WPR = K::WPR, TW = K::TW, JPT = K::JPT;
@@ -354,36 +356,96 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
     unsigned long long acc_total = 0;
     uint32_t g_cur = 0xffffffffu;
 
-    for (;;) {
-      unsigned long long c0 = 0;
-      if (lane == 0) c0 = atomicAdd(scr.work, (unsigned long long)chunk);
-      c0 = __shfl_sync(kFull, c0, 0);
-      if (c0 >= num_tiles) break;
-      const uint32_t c1 = (uint32_t)min(c0 + chunk, (unsigned long long)num_tiles);
-      uint32_t curI = 0xffffffffu;
-      ARow A{0, 0, 0, 0};
-      // the next tile's ids and sample words are loaded one tile ahead
-      uint32_t nI = row_indices[c0], nJL = indices[c0], nw0 = 0, nw1 = 0;
-      if constexpr (C == 128) {
-          const uint2 v = reinterpret_cast<const uint2*>(blocks + (size_t)c0 * TW)[lane];
-          nw0 = v.x;
-          nw1 = v.y;
-      } else {
-          if (lane < 16) nw0 = blocks[(size_t)c0 * TW + lane];
-      }
-      for (uint32_t t = (uint32_t)c0; t < c1; ++t) {
-        const uint32_t I = nI, JL = nJL, w0 = nw0, w1 = nw1;
-        if (t + 1 < c1) {
-            nI = row_indices[t + 1];
-            nJL = indices[t + 1];
-            if constexpr (C == 128) {
-                const uint2 v = reinterpret_cast<const uint2*>(blocks + (size_t)(t + 1) * TW)[lane];
-                nw0 = v.x;
-                nw1 = v.y;
-            } else {
-                if (lane < 16) nw0 = blocks[(size_t)(t + 1) * TW + lane];
-            }
+    // Tile queue over one word.  Grab k is a run of consecutive tiles.  When no row
+    // block holds more than four times the mean number of tiles plus 8 (meshes,
+    // Erdos-Renyi: tile costs alike), the schedule is guided: `chunk` tiles in the first
+    // grid-wide round of grabs, half as many in each later round, down to single tiles.
+    // Otherwise (power-law graphs, where a run of tiles can cost many times another) every
+    // grab is `chunk_skewed` tiles.  A warp asks for its next grab while it counts the
+    // last tile of the current one, so it never holds more than one grab.
+    const unsigned long long nwarps = (unsigned long long)gridDim.x * kWarps;
+    bool guided = false;
+    if (row_max) {
+        const uint64_t mx = __ldg(row_max);
+        guided = mx * (uint64_t)R <= 4ull * num_tiles + 8ull * (uint64_t)R;
+    }
+    if (!guided) chunk = chunk_skewed;
+    auto grab_range = [&](unsigned long long k, uint32_t& b, uint32_t& e) {
+        unsigned long long off = 0;
+        uint32_t sz = chunk;
+        while (guided && sz > 1 && k >= nwarps) {
+            off += nwarps * sz;
+            k -= nwarps;
+            sz >>= 1;
         }
+        off += k * sz;
+        b = off < num_tiles ? (uint32_t)off : num_tiles;
+        e = (uint32_t)min(off + sz, (unsigned long long)num_tiles);
+    };
+    // A tile's ids and sample words.
+    auto load_ids = [&](uint32_t t, uint32_t& tI, uint32_t& tJL, uint32_t& x0, uint32_t& x1) {
+        tI = row_indices[t];
+        tJL = indices[t];
+        if constexpr (C == 128) {
+            const uint2 v = reinterpret_cast<const uint2*>(blocks + (size_t)t * TW)[lane];
+            x0 = v.x;
+            x1 = v.y;
+        } else {
+            x0 = lane < 16 ? blocks[(size_t)t * TW + lane] : 0u;
+            x1 = 0u;
+        }
+    };
+    // A tile's indptr words: lane j <= JPT holds indptr[J_L*JPT + j] (the row blocks
+    // J_out of its slices), lanes 16 and 17 hold indptr[I] and indptr[I + 1].
+    auto load_ptrs = [&](uint32_t tI, uint32_t tJL) -> uint32_t {
+        if (lane <= JPT) {
+            const int64_t J = (int64_t)tJL * JPT + lane;
+            return indptr[J < R ? J : R];
+        }
+        if (lane == 16 || lane == 17) return indptr[tI + (uint32_t)(lane - 16)];
+        return 0u;
+    };
+
+    uint32_t curI = 0xffffffffu;
+    ARow A{0, 0, 0, 0, 0, 0};
+    uint32_t t, ce;  // current tile and the end of its grab
+    {
+        unsigned long long k = 0;
+        if (lane == 0) k = atomicAdd(scr.work, 1ull);
+        grab_range(__shfl_sync(kFull, k, 0), t, ce);
+    }
+    uint32_t I = 0, JL = 0, w0 = 0, w1 = 0, ptrs = 0;
+    if (t < num_tiles) {
+        load_ids(t, I, JL, w0, w1);
+        ptrs = load_ptrs(I, JL);
+    }
+    while (t < num_tiles) {
+        // The next tile: inside the grab its ids are loaded now and its indptr words once
+        // this tile's search has issued its loads; after the grab's last tile the queue
+        // atomic is issued now and read once this tile's search is under way.
+        uint32_t tn = t + 1, cen = ce;
+        uint32_t nI = 0, nJL = 0, nw0 = 0, nw1 = 0, nptrs = 0;
+        // 0: next ids loading; 1: and its indptr words; 2: queue atomic in flight;
+        // 3: grab resolved, ids loading (indptr words loaded at the top of the next tile)
+        int nstate;
+        unsigned long long kq = 0;
+        if (tn < ce) {
+            load_ids(tn, nI, nJL, nw0, nw1);
+            nstate = 0;
+        } else {
+            if (lane == 0) kq = atomicAdd(scr.work, 1ull);
+            nstate = 2;
+        }
+        auto next_ready = [&]() {
+            if (nstate == 2) {
+                grab_range(__shfl_sync(kFull, kq, 0), tn, cen);
+                if (tn < num_tiles) load_ids(tn, nI, nJL, nw0, nw1);
+                nstate = 3;
+            } else if (nstate == 0) {
+                nptrs = load_ptrs(nI, nJL);
+                nstate = 1;
+            }
+        };
 
         // ---- sample tile and its slices -------------------------------------
         const int nnz = (int)__reduce_add_sync(kFull, (unsigned)(__popc(w0) + __popc(w1)));
@@ -406,7 +468,8 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
         }
 
         if (I != curI) {
-            A = stage_row<C>(s, indptr, indices, I, lane);
+            const uint32_t a0 = __shfl_sync(kFull, ptrs, 16), a1 = __shfl_sync(kFull, ptrs, 17);
+            A = stage_row<C>(s, indices, a0, a1 - a0, lane);
             curI = I;
             if (graph_counts) {
                 uint32_t lo = 0, hi = num_graphs;  // last g with graph_rows[g] <= I
@@ -421,10 +484,7 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
                 }
             }
         }
-        if (lane <= JPT) {
-            const int64_t J = (int64_t)JL * JPT + lane;
-            s.jptr[lane] = indptr[J < R ? J : R];
-        }
+        if (lane <= JPT) s.jptr[lane] = ptrs;
         __syncwarp();
 
         // unit prefix over active slices
@@ -447,36 +507,37 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
                 if (lane >= d) e += y;
             }
             e -= mine;
-            // Tiles with more than one round of list elements take the heavy path: rows
-            // and columns of S that carry bits, per slice (to drop matches and units whose
-            // tile rows are empty), and the two-direction search plan.  Small tiles skip
-            // both: a single round costs less than planning it.
-            const bool heavy = upre[JPT] > (uint32_t)kWarp;
-            const uint32_t* __restrict__ rmask_g = heavy ? rowmask : nullptr;
-            uint32_t rm[JPT], cm[JPT];
+            const uint32_t* __restrict__ rmask_g = nullptr;
+            if constexpr (kHeavy) {
+                // Tiles with more than one round of list elements take the heavy path:
+                // rows and columns of S that carry bits, per slice (to drop matches and
+                // units whose tile rows are empty), and the two-direction search plan.
+                // Small tiles skip both: a single round costs less than planning it.
+                const bool heavy = upre[JPT] > (uint32_t)kWarp;
+                rmask_g = heavy ? rowmask : nullptr;
+                uint32_t rm[JPT], cm[JPT];
 #pragma unroll
-            for (int j = 0; j < JPT; ++j) rm[j] = cm[j] = 0xFFFFu;
-            if (!heavy) {
-            } else if constexpr (C == 128) {
+                for (int j = 0; j < JPT; ++j) rm[j] = cm[j] = 0xFFFFu;
+                if (!heavy) {
+                } else if constexpr (C == 128) {
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const uint32_t sl = ((q < 2 ? w0 : w1) >> (16 * (q & 1))) & 0xFFFFu;
-                    const unsigned bl = __ballot_sync(kFull, sl != 0);
-                    rm[q] = compress_even(bl);
-                    rm[4 + q] = compress_even(bl >> 1);
-                    cm[q] = __reduce_or_sync(kFull, (lane & 1) ? 0u : sl);
-                    cm[4 + q] = __reduce_or_sync(kFull, (lane & 1) ? sl : 0u);
+                    for (int q = 0; q < 4; ++q) {
+                        const uint32_t sl = ((q < 2 ? w0 : w1) >> (16 * (q & 1))) & 0xFFFFu;
+                        const unsigned bl = __ballot_sync(kFull, sl != 0);
+                        rm[q] = compress_even(bl);
+                        rm[4 + q] = compress_even(bl >> 1);
+                        cm[q] = __reduce_or_sync(kFull, (lane & 1) ? 0u : sl);
+                        cm[4 + q] = __reduce_or_sync(kFull, (lane & 1) ? sl : 0u);
+                    }
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 2; ++q) {
+                        const uint32_t sl = (w0 >> (16 * q)) & 0xFFFFu;
+                        rm[q] = __ballot_sync(kFull, sl != 0) & 0xFFFFu;
+                        cm[q] = __reduce_or_sync(kFull, sl);
+                    }
                 }
-            } else {
-#pragma unroll
-                for (int q = 0; q < 2; ++q) {
-                    const uint32_t sl = (w0 >> (16 * q)) & 0xFFFFu;
-                    rm[q] = __ballot_sync(kFull, sl != 0) & 0xFFFFu;
-                    cm[q] = __reduce_or_sync(kFull, sl);
-                }
-            }
-            // search plan: lane j < JPT picks slice j's direction and list
-            {
+                // search plan: lane j < JPT picks slice j's direction and list
                 uint32_t len = 0, start = 0, dir = 0;
                 if (lane < JPT && ((active >> lane) & 1u)) {
                     const uint32_t jb = s.jptr[lane], je = s.jptr[lane + 1];
@@ -496,15 +557,17 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
                 }
 #pragma unroll
                 for (int j = 0; j < JPT; ++j) upre[j + 1] = upre[j] + __shfl_sync(kFull, len, j);
+                if (lane == 0) {
+#pragma unroll
+                    for (int j = 0; j < JPT; ++j) {
+                        s.rmask[j] = (uint16_t)rm[j];
+                        s.cmask[j] = (uint16_t)cm[j];
+                    }
+                }
             }
             if (lane == 0) {
 #pragma unroll
                 for (int j = 0; j <= JPT; ++j) s.upre[j] = upre[j];
-#pragma unroll
-                for (int j = 0; j < JPT; ++j) {
-                    s.rmask[j] = (uint16_t)rm[j];
-                    s.cmask[j] = (uint16_t)cm[j];
-                }
             }
             __syncwarp();
             const uint32_t W = upre[JPT];
@@ -522,22 +585,27 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
                             us = upre[j];
                             jsel = j;
                         }
-                    const uint32_t idx = s.sstart[jsel] + (u - us);
-                    if (!s.sdir[jsel]) {
-                        pb = idx;
+                    if constexpr (!kHeavy) {
+                        pb = s.jptr[jsel] + (u - us);
                         found = a_lookup<C>(s, A, indices, indices[pb], pa);
                     } else {
-                        pa = idx;
-                        const uint32_t a = indices[pa];
-                        const uint64_t cw = (uint64_t)(JL * JPT + jsel) * cell_wpr + (a >> 5);
-                        const uint32_t x = cellbm[cw], bit = 1u << (a & 31u);
-                        found = (x & bit) != 0u;
-                        if (found) pb = cellpre[cw] + __popc(x & (bit - 1u));
-                    }
-                    if (found && rmask_g) {
-                        ra = rmask_g[pa];
-                        rb = rmask_g[pb];
-                        found = (ra & s.rmask[jsel]) && (rb & s.cmask[jsel]);
+                        const uint32_t idx = s.sstart[jsel] + (u - us);
+                        if (!s.sdir[jsel]) {
+                            pb = idx;
+                            found = a_lookup<C>(s, A, indices, indices[pb], pa);
+                        } else {
+                            pa = idx;
+                            const uint32_t a = indices[pa];
+                            const uint64_t cw = (uint64_t)(JL * JPT + jsel) * cell_wpr + (a >> 5);
+                            const uint32_t x = cellbm[cw], bit = 1u << (a & 31u);
+                            found = (x & bit) != 0u;
+                            if (found) pb = cellpre[cw] + __popc(x & (bit - 1u));
+                        }
+                        if (found && rmask_g) {
+                            ra = rmask_g[pa];
+                            rb = rmask_g[pb];
+                            found = (ra & s.rmask[jsel]) && (rb & s.cmask[jsel]);
+                        }
                     }
                 }
                 const unsigned mb = __ballot_sync(kFull, found);
@@ -545,8 +613,10 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
                     const uint32_t k = nm - lo + __popc(mb & lt);
                     s.mpa[k] = pa;
                     s.mpb[k] = pb;
-                    s.mra[k] = (uint16_t)ra;
-                    s.mrb[k] = (uint16_t)rb;
+                    if constexpr (kHeavy) {
+                        s.mra[k] = (uint16_t)ra;
+                        s.mrb[k] = (uint16_t)rb;
+                    }
                 }
                 if (lane <= JPT) {
                     const uint32_t lim = s.upre[lane];
@@ -556,14 +626,16 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
                 }
                 nm += __popc(mb);
                 if (nm - lo > (uint32_t)(kMCap - kWarp) || (ub + kWarp >= W && nm > lo)) {
+                    next_ready();
                     if (lane <= JPT) s.mc[lane] = mc;
                     __syncwarp();
-                    acc += bit_pass<C>(s, w0, w1, e, (uint32_t)nnz, lo, nm, blocks, lane);
+                    acc += bit_pass<C, kHeavy>(s, w0, w1, e, (uint32_t)nnz, lo, nm, blocks, lane);
                     lo = nm;
                 }
             }
         } else {
             // ================= dense path: binary tensor core ================
+            next_ready();
             if constexpr (C == 128) {
                 s.S[2 * lane] = w0;
                 s.S[2 * lane + 1] = w1;
@@ -634,8 +706,15 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
                 acc += (unsigned long long)part;
             }
         }
+        next_ready();
         __syncwarp();
-      }
+        t = tn;
+        ce = cen;
+        I = nI;
+        JL = nJL;
+        w0 = nw0;
+        w1 = nw1;
+        ptrs = nstate == 1 ? nptrs : (t < num_tiles ? load_ptrs(I, JL) : 0u);
     }
 
     if (graph_counts) {
@@ -683,9 +762,9 @@ int count_grid_size(int tile_cols)
     int per_sm = 0;
     cudaError_t e;
     if (tile_cols == 128)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_count<128>, kThreads, 0);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_count<128, false>, kThreads, 0);
     else
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_count<32>, kThreads, 0);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_count<32, false>, kThreads, 0);
     if (e != cudaSuccess || per_sm < 1) per_sm = 1;
     return per_sm * device_sm_count();
 }
@@ -695,25 +774,40 @@ int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
                  int32_t n_row_blocks, int tau, CountScratch scr, cudaStream_t s,
                  const uint32_t* graph_rows, uint32_t num_graphs, unsigned long long* graph_counts,
                  const uint32_t* rowmask, const uint32_t* cellbm, const uint32_t* cellpre,
-                 uint64_t cell_wpr)
+                 uint64_t cell_wpr, const uint32_t* row_max)
 {
     const int grid = count_grid_size(tile_cols);
-    // About eight queue grabs per warp, between 8 and 64 consecutive tiles per grab: the
-    // queue head is one word, and every grab is an atomic on it.
+    // Guided schedule: the first round of grabs is about half of an even share per warp
+    // (1 to 64 tiles).  Fixed schedule: about an eighth of an even share (8 to 64 tiles);
+    // a grab of a power-law graph's row block often holds tiles of one long list, which
+    // is staged once per grab.
     const uint64_t warps = (uint64_t)grid * kWarps;
-    uint64_t chunk = num_tiles / (warps * 8);
-    if (chunk < 8) chunk = 8;
-    if (chunk > 64) chunk = 64;
-    if (tile_cols == 128)
-        k_count<128><<<grid, kThreads, 0, s>>>(indptr, indices, row_indices, blocks, num_tiles,
-                                               n_row_blocks, tau, (uint32_t)chunk, scr,
-                                               graph_rows, num_graphs, graph_counts, rowmask,
-                                               cellbm, cellpre, cell_wpr);
-    else
-        k_count<32><<<grid, kThreads, 0, s>>>(indptr, indices, row_indices, blocks, num_tiles,
-                                              n_row_blocks, tau, (uint32_t)chunk, scr, graph_rows,
-                                              num_graphs, graph_counts, rowmask, cellbm, cellpre,
-                                              cell_wpr);
+    uint64_t chunk = num_tiles / (warps * 2), chunk_s = num_tiles / (warps * 8);
+    chunk = chunk < 1 ? 1 : (chunk > 64 ? 64 : chunk);
+    chunk_s = chunk_s < 8 ? 8 : (chunk_s > 64 ? 64 : chunk_s);
+    // The occupancy masks and the two-direction search pay off only where row blocks
+    // hold many tiles (long lists to search); meshes and stencils (a few tiles per row
+    // block) take the light kernel.
+    const bool heavy = rowmask != nullptr && n_row_blocks > 0 &&
+                       (uint64_t)num_tiles >= 8ull * (uint64_t)n_row_blocks;
+    if (!heavy) {
+        rowmask = nullptr;
+        cellbm = cellpre = nullptr;
+    }
+#define BTC_LAUNCH_COUNT(CC, HH)                                                              \
+    k_count<CC, HH><<<grid, kThreads, 0, s>>>(indptr, indices, row_indices, blocks, num_tiles, \
+                                              n_row_blocks, tau, (uint32_t)chunk, scr,         \
+                                              graph_rows, num_graphs, graph_counts, rowmask,   \
+                                              cellbm, cellpre, cell_wpr, (uint32_t)chunk_s, \
+                                              row_max)
+    if (tile_cols == 128) {
+        if (heavy) BTC_LAUNCH_COUNT(128, true);
+        else BTC_LAUNCH_COUNT(128, false);
+    } else {
+        if (heavy) BTC_LAUNCH_COUNT(32, true);
+        else BTC_LAUNCH_COUNT(32, false);
+    }
+#undef BTC_LAUNCH_COUNT
     return cudaGetLastError() == cudaSuccess ? BTC_OK : BTC_E_CUDA;
 }
 
