@@ -155,7 +155,7 @@ def launches_per_step(n: int, tile_cols: int, orient_degree: bool, m: int) -> in
     if orient_degree:
         db = min(32, max(1, (2 * m).bit_length()))
         k += 1 + 1 + 1 + 3 * (-(-db // 8)) + 1  # degree, rank keys, set count, sort, scatter
-    return k + 1  # count
+    return k + 1 + 1  # row-occupancy masks, count
 
 
 def cpu_reference(rowptr, col, m_lower, budget_s=10.0):
@@ -432,6 +432,10 @@ def main():
     ap.add_argument("--requests", type=int, default=2000, help="serve workload: requests per rate")
     ap.add_argument("--rates", default="50,200,1000,5000", help="serve workload: arrivals/s")
     ap.add_argument("--large-frac", type=float, default=0.05, help="serve workload: large share")
+    ap.add_argument("--shard", action="store_true",
+                    help="one graph per job: every rank counts a cost-balanced tile range of the "
+                         "same Bit-BSR and the counts are all-reduced (strong scaling); default: "
+                         "one graph per rank (weak scaling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -483,10 +487,22 @@ def main():
     tw_bytes = 2 * tile  # 16 rows x tile bits / 8
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
     d_out = torch.zeros(1, dtype=torch.int64, device="cuda")
+    # --shard: every rank holds the whole Bit-BSR and counts its tile range; one int64
+    # all-reduce (NCCL) adds the ranges.  The bounds depend only on the graph.
+    bounds = g.partition(world, stream=stream) if args.shard else None
+    jobs = 1 if args.shard else world  # graphs counted per step, all ranks together
+
+    def count_step(out):
+        if args.shard:
+            g.count_tiles(bounds[rank], bounds[rank + 1], stream=stream, out=out)
+            if dist:
+                dist.all_reduce(out)
+        else:
+            g.count_async(stream=stream, d_out=out.data_ptr())
 
     def step_device():
         g.rebuild(d_src, d_dst, n, tile, orient_degree=odeg, stream=stream)
-        g.count_async(stream=stream, d_out=d_out.data_ptr())
+        count_step(d_out)
 
     for _ in range(args.warmup):
         flush.zero_()
@@ -552,7 +568,11 @@ def main():
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         g.rebuild(np_src, np_dst, n, tile, orient_degree=odeg, stream=stream)
-        cnt = g.count(stream=stream)
+        if args.shard:
+            count_step(d_out)
+            cnt = int(d_out.item())
+        else:
+            cnt = g.count(stream=stream)
         e1.record(stream)
         e1.synchronize()
         assert cnt == expected
@@ -568,31 +588,36 @@ def main():
     bytes_count = 4 * (R + 1) + 8 * B + tw_bytes * B + 8
     bytes_build = 8 * m_in + 4 * (R + 1) + 8 * B + tw_bytes * B
     achieved = bytes_count / tc / 1e9
+    # DRAM bytes of one count launch, from the committed ncu summary of this workload
+    # (dram__bytes_read.sum + dram__bytes_write.sum; a line "dram_bytes_per_launch: N")
     traffic = None
-    prof = os.path.join(ROOT, "profiles", f"count_{tile}_{args.workload}.json")
+    prof = os.path.join(ROOT, "profiles", f"count_{tile}_{args.workload}.md")
     if os.path.exists(prof):
         with open(prof) as f:
-            traffic = json.load(f).get("dram_bytes_per_launch")
+            for ln in f:
+                if ln.startswith("dram_bytes_per_launch:"):
+                    traffic = int(ln.split(":", 1)[1])
 
     line = {
         "metric": METRIC,
-        "value": world * m_lower * args.steps / (total_ms / 1e3),
+        "value": jobs * m_lower * args.steps / (total_ms / 1e3),
         "unit": UNIT,
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps,
         "higher_is_better": True,
-        "scaling": "weak",
+        "scaling": "strong" if args.shard else "weak",
         "vs_baseline": None,
         "dtype": "int32",
         "data": "synthetic",
         "config": {"workload": meta["workload"], "vertices": n, "edges": m_lower,
                    "input_pairs": m_in, "tile": f"16x{tile}", "tiles": B, "triangles": expected,
                    "orientation": "descending degree" if odeg else "natural id",
-                   "parallelism": f"replica x{world}" if world > 1 else "single GPU",
+                   "parallelism": (f"tile-sharded x{world}, int64 all-reduce" if args.shard
+                                   else f"replica x{world}" if world > 1 else "single GPU"),
                    "l2": "flushed before every timed step (512 MB write)"},
-        "e2e": {"value": world * m_lower * e2e_steps / (e2e_total / 1e3), "unit": UNIT,
+        "e2e": {"value": jobs * m_lower * e2e_steps / (e2e_total / 1e3), "unit": UNIT,
                 "h2d_bytes_per_step": 8 * m_in, "d2h_bytes_per_step": 8 + 24},
         "gpu_launches": launches_per_step(n, tile, odeg, m_in) * args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",

@@ -57,6 +57,9 @@ EXPORTS = [
     "btc_server_poll",
     "btc_server_stats_get",
     "btc_server_destroy",
+    "btc_partition_tiles",
+    "btc_partition_from_costs",
+    "btc_count_tiles_async",
 ]
 
 
@@ -167,6 +170,9 @@ def lib():
         L.btc_server_stats_get.argtypes = [vp, P(BtcServerStats)]
         L.btc_server_destroy.argtypes = [vp]
         L.btc_server_destroy.restype = None
+        L.btc_partition_tiles.argtypes = [vp, C.c_int, vp, vp]
+        L.btc_partition_from_costs.argtypes = [vp, C.c_uint64, u32, u32, C.c_int, vp]
+        L.btc_count_tiles_async.argtypes = [vp, u32, u32, C.c_int, vp, vp]
         for name in EXPORTS:
             if name not in ("btc_bcsr_free", "btc_free", "btc_strerror", "btc_batch_free",
                             "btc_server_default_config", "btc_server_destroy"):

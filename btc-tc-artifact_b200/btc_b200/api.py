@@ -294,6 +294,26 @@ class BitBSR:
     def count_async(self, tau: int = _lib.BTC_TAU_DEFAULT, stream=None, d_out: int | None = None):
         check(lib().btc_count_async(self._h, int(tau), _stream_ptr(stream), d_out), "btc_count_async")
 
+    def partition(self, parts: int, stream=None) -> list[int]:
+        """Tile bounds [b_0 = 0, ..., b_parts = num_tiles] of `parts` ranges of about equal
+        estimated count cost (btc_partition_tiles)."""
+        b = np.zeros(int(parts) + 1, np.uint32)
+        check(lib().btc_partition_tiles(self._h, int(parts), _stream_ptr(stream), b.ctypes.data),
+              "btc_partition_tiles")
+        return [int(x) for x in b]
+
+    def count_tiles(self, tile_begin: int, tile_end: int, tau: int = _lib.BTC_TAU_DEFAULT,
+                    stream=None, out=None):
+        """Enqueues the count of sample tiles [tile_begin, tile_end) into `out`, a one-element
+        int64 CUDA tensor (made on the current device when None), and returns `out`."""
+        import torch
+        if out is None:
+            out = torch.zeros(1, dtype=torch.int64, device=f"cuda:{torch.cuda.current_device()}")
+        check(lib().btc_count_tiles_async(self._h, int(tile_begin), int(tile_end), int(tau),
+                                          _stream_ptr(stream), out.data_ptr()),
+              "btc_count_tiles_async")
+        return out
+
     def info(self) -> _lib.BtcBitbsrView:
         v = _lib.BtcBitbsrView()
         check(lib().btc_bitbsr_info(self._h, C.byref(v)), "btc_bitbsr_info")

@@ -5,6 +5,9 @@ tau (a tile takes the binary tensor-core path when its popcount exceeds tau), th
 experiment apps/tau_sweep.cu:410-566 runs for the reference, here checking every tau
 against the first one.  ``python btc-tc-artifact_b200/btc_b200/tune.py`` runs the sweep
 on the standard graphs and prints a markdown table (microseconds per launch).
+
+``tune.py --count GRAPH --tile C [--reps K]`` builds one standard graph and counts it K
+times (default tau), printing the counts: a fixed target for profilers.
 """
 from __future__ import annotations
 
@@ -31,17 +34,41 @@ def tau_sweep(g, taus=TAUS, reps: int = 30) -> dict:
     return out
 
 
-def standard_graphs():
+def standard_graphs(names=None):
     from . import graphs as G
-    return [("stencil27_64", G.stencil27(64), False),
-            ("er_16384_16", G.erdos_renyi(16384, 16, seed=1), False),
-            ("rmat18_deg", G.rmat(18, 16, seed=7), True)]
+    makers = {"stencil27_64": lambda: G.stencil27(64),
+              "er_16384_16": lambda: G.erdos_renyi(16384, 16, seed=1),
+              "rmat18_deg": lambda: G.rmat(18, 16, seed=7),
+              "rmat20_deg": lambda: G.rmat(20, 16, seed=7)}
+    names = names or ["stencil27_64", "er_16384_16", "rmat18_deg"]
+    return [(k, makers[k](), k.endswith("_deg")) for k in names]
 
 
-def main() -> None:
+def count_once(name: str, tile: int, reps: int) -> None:
     import torch
 
     from .api import BitBSR
+    [(_, (s, d, n), deg)] = standard_graphs([name])
+    g = BitBSR(torch.from_numpy(s).cuda(), torch.from_numpy(d).cuda(), n, tile,
+               orient_degree=deg)
+    print(name, f"16x{tile}", g.num_tiles, [g.count() for _ in range(reps)], flush=True)
+    g.free()
+
+
+def main() -> None:
+    import argparse
+
+    import torch
+
+    from .api import BitBSR
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--count", default=None, help="count one standard graph instead of the sweep")
+    ap.add_argument("--tile", type=int, default=128)
+    ap.add_argument("--reps", type=int, default=3)
+    args = ap.parse_args()
+    if args.count:
+        count_once(args.count, args.tile, args.reps)
+        return
     print("| graph | tile | tiles | " + " | ".join(
         "all-sparse" if t == 0x7FFFFFFF else f"tau={t}" for t in TAUS) + " |")
     print("|---|---|---|" + "---|" * len(TAUS))

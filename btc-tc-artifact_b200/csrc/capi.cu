@@ -223,7 +223,8 @@ static int build_into(btc_bitbsr* g, const int32_t* src, const int32_t* dst, int
     return BTC_OK;
 }
 
-int count_handle(btc_bitbsr* g, int tau, cudaStream_t s, unsigned long long* d_out2)
+int count_handle(btc_bitbsr* g, int tau, cudaStream_t s, unsigned long long* d_out2,
+                 uint32_t tile_begin, uint32_t tile_end)
 {
     if (!g) return BTC_E_INVAL;
     if (tau == BTC_TAU_DEFAULT) tau = default_tau(g->tile_cols);
@@ -239,7 +240,7 @@ int count_handle(btc_bitbsr* g, int tau, cudaStream_t s, unsigned long long* d_o
                         g->used_bitmap ? g->bitmap.as<uint32_t>() : nullptr,
                         g->used_bitmap ? g->prefix.as<uint32_t>() : nullptr,
                         bitmap_words_per_row(make_geom(g->n, g->tile_cols)),
-                        g->rowmask.as<uint32_t>() + g->num_tiles);
+                        g->rowmask.as<uint32_t>() + g->num_tiles, tile_begin, tile_end);
 }
 
 // ===========================================================================

@@ -152,7 +152,8 @@ int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
                  const uint32_t* graph_rows = nullptr, uint32_t num_graphs = 0,
                  unsigned long long* graph_counts = nullptr, const uint32_t* rowmask = nullptr,
                  const uint32_t* cellbm = nullptr, const uint32_t* cellpre = nullptr,
-                 uint64_t cell_wpr = 0, const uint32_t* row_max = nullptr);
+                 uint64_t cell_wpr = 0, const uint32_t* row_max = nullptr,
+                 uint32_t tile_begin = 0, uint32_t tile_end = 0xffffffffu);
 
 // rowmask[t] bit r = tile t's row r has a bit (built after the tiles are filled), and
 // rowmask[num_tiles] = the most tiles in one row block (indptr's largest step), which

@@ -332,7 +332,8 @@ template <int C, bool kHeavy>
 __global__ void __launch_bounds__(kThreads, 4)
 k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
         const uint32_t* __restrict__ row_indices, const uint32_t* __restrict__ blocks,
-        uint32_t num_tiles, int32_t R, int tau, uint32_t chunk, CountScratch scr,
+        uint32_t num_tiles, uint32_t tile_begin, uint32_t tile_end, int32_t R, int tau,
+        uint32_t chunk, CountScratch scr,
         const uint32_t* __restrict__ graph_rows, uint32_t num_graphs,
         unsigned long long* __restrict__ graph_counts, const uint32_t* __restrict__ rowmask,
         const uint32_t* __restrict__ cellbm, const uint32_t* __restrict__ cellpre, uint64_t cell_wpr,
@@ -379,8 +380,9 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
             sz >>= 1;
         }
         off += k * sz;
-        b = off < num_tiles ? (uint32_t)off : num_tiles;
-        e = (uint32_t)min(off + sz, (unsigned long long)num_tiles);
+        const unsigned long long span = tile_end - tile_begin;
+        b = tile_begin + (uint32_t)(off < span ? off : span);
+        e = tile_begin + (uint32_t)min(off + sz, span);
     };
     // A tile's ids and sample words.
     auto load_ids = [&](uint32_t t, uint32_t& tI, uint32_t& tJL, uint32_t& x0, uint32_t& x1) {
@@ -415,11 +417,11 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
         grab_range(__shfl_sync(kFull, k, 0), t, ce);
     }
     uint32_t I = 0, JL = 0, w0 = 0, w1 = 0, ptrs = 0;
-    if (t < num_tiles) {
+    if (t < tile_end) {
         load_ids(t, I, JL, w0, w1);
         ptrs = load_ptrs(I, JL);
     }
-    while (t < num_tiles) {
+    while (t < tile_end) {
         // The next tile: inside the grab its ids are loaded now and its indptr words once
         // this tile's search has issued its loads; after the grab's last tile the queue
         // atomic is issued now and read once this tile's search is under way.
@@ -439,7 +441,7 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
         auto next_ready = [&]() {
             if (nstate == 2) {
                 grab_range(__shfl_sync(kFull, kq, 0), tn, cen);
-                if (tn < num_tiles) load_ids(tn, nI, nJL, nw0, nw1);
+                if (tn < tile_end) load_ids(tn, nI, nJL, nw0, nw1);
                 nstate = 3;
             } else if (nstate == 0) {
                 nptrs = load_ptrs(nI, nJL);
@@ -714,7 +716,7 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
         JL = nJL;
         w0 = nw0;
         w1 = nw1;
-        ptrs = nstate == 1 ? nptrs : (t < num_tiles ? load_ptrs(I, JL) : 0u);
+        ptrs = nstate == 1 ? nptrs : (t < tile_end ? load_ptrs(I, JL) : 0u);
     }
 
     if (graph_counts) {
@@ -774,15 +776,19 @@ int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
                  int32_t n_row_blocks, int tau, CountScratch scr, cudaStream_t s,
                  const uint32_t* graph_rows, uint32_t num_graphs, unsigned long long* graph_counts,
                  const uint32_t* rowmask, const uint32_t* cellbm, const uint32_t* cellpre,
-                 uint64_t cell_wpr, const uint32_t* row_max)
+                 uint64_t cell_wpr, const uint32_t* row_max, uint32_t tile_begin,
+                 uint32_t tile_end)
 {
+    if (tile_end > num_tiles) tile_end = num_tiles;
+    if (tile_begin > tile_end) tile_begin = tile_end;
+    const uint32_t span = tile_end - tile_begin;
     const int grid = count_grid_size(tile_cols);
     // Guided schedule: the first round of grabs is about half of an even share per warp
     // (1 to 64 tiles).  Fixed schedule: about an eighth of an even share (8 to 64 tiles);
     // a grab of a power-law graph's row block often holds tiles of one long list, which
     // is staged once per grab.
     const uint64_t warps = (uint64_t)grid * kWarps;
-    uint64_t chunk = num_tiles / (warps * 2), chunk_s = num_tiles / (warps * 8);
+    uint64_t chunk = span / (warps * 2), chunk_s = span / (warps * 8);
     chunk = chunk < 1 ? 1 : (chunk > 64 ? 64 : chunk);
     chunk_s = chunk_s < 8 ? 8 : (chunk_s > 64 ? 64 : chunk_s);
     // The occupancy masks and the two-direction search pay off only where row blocks
@@ -796,7 +802,8 @@ int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
     }
 #define BTC_LAUNCH_COUNT(CC, HH)                                                              \
     k_count<CC, HH><<<grid, kThreads, 0, s>>>(indptr, indices, row_indices, blocks, num_tiles, \
-                                              n_row_blocks, tau, (uint32_t)chunk, scr,         \
+                                              tile_begin, tile_end, n_row_blocks, tau,         \
+                                              (uint32_t)chunk, scr,                            \
                                               graph_rows, num_graphs, graph_counts, rowmask,   \
                                               cellbm, cellpre, cell_wpr, (uint32_t)chunk_s, \
                                               row_max)

@@ -48,4 +48,7 @@ enum { kMetaValid = 0, kMetaBad = 1, kMetaTiles = 2, kMetaUniq = 3, kMetaN = 4, 
 
 int default_tau(int tile_cols);
 int ensure_count_scratch(btc_bitbsr* g);
-int count_handle(btc_bitbsr* g, int tau, cudaStream_t s, unsigned long long* d_out2);
+// Counts tiles [tile_begin, tile_end) (clamped to the tile count) into g->result and,
+// when d_out2 is given, *d_out2.
+int count_handle(btc_bitbsr* g, int tau, cudaStream_t s, unsigned long long* d_out2,
+                 uint32_t tile_begin = 0, uint32_t tile_end = 0xffffffffu);

@@ -180,6 +180,31 @@ BTC_API int btc_count_bcsr_noalloc(const btc_bcsr_device* bcsr, int tile_cols, i
  * stream reaches it. */
 BTC_API int btc_count_async(btc_bitbsr* g, int tau, btc_stream_t stream, unsigned long long* d_out);
 
+/* ---- one graph on several GPUs ------------------------------------------------
+ * No counterpart in the reference, which counts on one GPU.  Every rank builds the
+ * same Bit-BSR (same input and flags, hence the same tiles in the same order), takes
+ * its tile range from btc_partition_tiles, counts it with btc_count_tiles_async, and
+ * the ranks add their counts (one int64 all-reduce).  The counts of any partition of
+ * [0, num_tiles) add up to btc_count's result. */
+
+/* bounds[0..parts]: tile ranges [bounds[r], bounds[r+1]) of about equal estimated count
+ * cost, cut at multiples of 256 tiles.  One device pass over the tiles and one wait on
+ * `stream`; allocates (and frees) 8 bytes per 256 tiles. */
+BTC_API int btc_partition_tiles(const btc_bitbsr* g, int parts, btc_stream_t stream,
+                                uint32_t* bounds);
+
+/* The host half of btc_partition_tiles: bounds from per-bucket costs (bucket b holds
+ * tiles [b*bucket_tiles, (b+1)*bucket_tiles)).  Needs no GPU. */
+BTC_API int btc_partition_from_costs(const unsigned long long* bucket_cost, uint64_t n_buckets,
+                                     uint32_t bucket_tiles, uint32_t num_tiles, int parts,
+                                     uint32_t* bounds);
+
+/* Counts the sample tiles [tile_begin, tile_end) into device memory at d_out, enqueued
+ * on `stream` without waiting.  Uses the handle's count scratch: one count at a time
+ * per handle. */
+BTC_API int btc_count_tiles_async(btc_bitbsr* g, uint32_t tile_begin, uint32_t tile_end, int tau,
+                                  btc_stream_t stream, unsigned long long* d_out);
+
 /* Fills *v with the handle's arrays and sizes. */
 BTC_API int btc_bitbsr_info(const btc_bitbsr* g, btc_bitbsr_view* v);
 

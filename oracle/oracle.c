@@ -22,6 +22,8 @@
  *                        every 16-row block J_out covered by S's columns, every K
  *                        common to rows I and J_out: sum over mask bits (r,c) of S of
  *                        popc(L[I,K][r] & L[J_out,K][c])).  Accumulates in uint64.
+ *   orc_bitbsr_count_range  the same sum over a range of sample tiles (the unit a rank
+ *                        of a multi-GPU count takes).
  *
  * Parity pin: counts are pinned against the reference's own CPU path
  * (triangle_count_cpu.h compiled from the reference headers by oracle/ref/Makefile)
@@ -238,19 +240,20 @@ void orc_bitbsr_density_hist(const uint32_t* blocks, int64_t B, int C, int64_t* 
 /* Bit-BSR count (tc_16x128_mma_v5.h:9-211, tc_16x32_mma_v6.h:9-238)         */
 /* ------------------------------------------------------------------------- */
 
-uint64_t orc_bitbsr_count(const uint32_t* indptr, const uint32_t* indices,
-                          const uint32_t* row_indices, const uint32_t* blocks,
-                          int32_t n, int64_t B, int C, int threads)
+/* Count of the sample tiles [t0, t1) alone; the counts of a partition of [0, B) add
+ * up to the whole count (each tile's term of the sum is independent of the others). */
+uint64_t orc_bitbsr_count_range(const uint32_t* indptr, const uint32_t* indices,
+                                const uint32_t* row_indices, const uint32_t* blocks,
+                                int32_t n, int64_t t0, int64_t t1, int C, int threads)
 {
     const int WPR = C / 32, TW = 16 * WPR, JPT = C / 16;
     const int32_t R = (n + 15) / 16;
     uint64_t total = 0;
-    (void)n;
 #ifdef _OPENMP
     if (threads > 0) omp_set_num_threads(threads);
 #pragma omp parallel for reduction(+ : total) schedule(dynamic, 64)
 #endif
-    for (int64_t s = 0; s < B; ++s) {
+    for (int64_t s = t0; s < t1; ++s) {
         const uint32_t I = row_indices[s], JL = indices[s];
         const uint32_t* S = blocks + (size_t)s * TW;
         for (int j = 0; j < JPT; ++j) {
@@ -288,4 +291,11 @@ uint64_t orc_bitbsr_count(const uint32_t* indptr, const uint32_t* indices,
         }
     }
     return total;
+}
+
+uint64_t orc_bitbsr_count(const uint32_t* indptr, const uint32_t* indices,
+                          const uint32_t* row_indices, const uint32_t* blocks,
+                          int32_t n, int64_t B, int C, int threads)
+{
+    return orc_bitbsr_count_range(indptr, indices, row_indices, blocks, n, 0, B, C, threads);
 }

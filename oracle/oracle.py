@@ -59,6 +59,9 @@ def lib():
         L.orc_bitbsr_density_hist.argtypes = [_u32p, C.c_int64, C.c_int, _i64p]
         L.orc_bitbsr_count.restype = C.c_uint64
         L.orc_bitbsr_count.argtypes = [_u32p, _u32p, _u32p, _u32p, C.c_int32, C.c_int64, C.c_int, C.c_int]
+        L.orc_bitbsr_count_range.restype = C.c_uint64
+        L.orc_bitbsr_count_range.argtypes = [_u32p, _u32p, _u32p, _u32p, C.c_int32, C.c_int64,
+                                             C.c_int64, C.c_int, C.c_int]
         _lib = L
     return _lib
 
@@ -114,6 +117,14 @@ def bitbsr_count(bsr, threads: int = 0) -> int:
     pad = lambda a: a if len(a) else np.zeros(1, np.uint32)
     return int(lib().orc_bitbsr_count(bsr["indptr"], pad(bsr["indices"]), pad(bsr["row_indices"]),
                                       pad(bsr["blocks"]), bsr["n"], B, bsr["tile_cols"], threads))
+
+
+def bitbsr_count_range(bsr, t0: int, t1: int, threads: int = 0) -> int:
+    """Count of the sample tiles [t0, t1) of an oracle Bit-BSR."""
+    pad = lambda a: a if len(a) else np.zeros(1, np.uint32)
+    return int(lib().orc_bitbsr_count_range(bsr["indptr"], pad(bsr["indices"]),
+                                            pad(bsr["row_indices"]), pad(bsr["blocks"]), bsr["n"],
+                                            int(t0), int(t1), bsr["tile_cols"], threads))
 
 
 def density_hist(bsr):
