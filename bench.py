@@ -148,7 +148,7 @@ def launches_per_step(n: int, tile_cols: int, orient_degree: bool, m: int) -> in
     ncb = (n + tile_cols - 1) // tile_cols
     bm_bytes = 4 * R * ((ncb + 31) // 32)
     if bm_bytes <= (4 << 30) and bm_bytes <= 32 * m + (64 << 20):
-        k = 6
+        k = 4  # mark, chunk count + scan, emit (+ zero tiles, last indptr), fill
     else:
         t_bits = max(R - 1, 0).bit_length() + max(ncb - 1, 0).bit_length()
         k = 1 + 3 * (-(-t_bits // 8)) + 2 + 1 + 1  # keys, sort, segment (2), fill, indptr
@@ -500,8 +500,10 @@ def main():
         else:
             g.count_async(stream=stream, d_out=out.data_ptr())
 
+    # a step enqueues the build and the count without a host wait (BTC_BUILD_ASYNC;
+    # the handle's arrays from the first build have room)
     def step_device():
-        g.rebuild(d_src, d_dst, n, tile, orient_degree=odeg, stream=stream)
+        g.rebuild(d_src, d_dst, n, tile, orient_degree=odeg, stream=stream, asynchronous=True)
         count_step(d_out)
 
     for _ in range(args.warmup):
@@ -567,7 +569,7 @@ def main():
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        g.rebuild(np_src, np_dst, n, tile, orient_degree=odeg, stream=stream)
+        g.rebuild(np_src, np_dst, n, tile, orient_degree=odeg, stream=stream, asynchronous=True)
         if args.shard:
             count_step(d_out)
             cnt = int(d_out.item())

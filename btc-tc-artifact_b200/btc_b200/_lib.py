@@ -16,10 +16,12 @@ BTC_E_NOMEM = -2
 BTC_E_CUDA = -3
 BTC_E_TIMEOUT = -4
 BTC_E_RANGE = -5
+BTC_E_CAPACITY = -6
 
 BTC_INPUT_ON_HOST = 0x1
 BTC_ORIENT_DEGREE = 0x2
 BTC_BUILD_RADIX = 0x4
+BTC_BUILD_ASYNC = 0x8
 BTC_TAU_DEFAULT = -1
 BTC_TAU_ALL_SPARSE = 0x7FFFFFFF
 

@@ -274,15 +274,21 @@ class BitBSR:
         self._keep = None
 
     def rebuild(self, src, dst, n: int, tile_cols: int = 0, orient_degree: bool = False,
-                stream=None, radix: bool = False) -> None:
+                stream=None, radix: bool = False, asynchronous: bool = False) -> None:
+        """Rebuild into this handle.  asynchronous=True enqueues the build without waiting
+        when the handle's arrays from the previous build have room (BTC_BUILD_ASYNC); its
+        status then comes with the next call that waits (count, info, ...).  The inputs
+        (and any converted copies, kept on the handle) must outlive the enqueued build."""
         sp, dp, m, flags, keep = _edge_ptrs(src, dst)
         if orient_degree:
             flags |= _lib.BTC_ORIENT_DEGREE
         if radix:
             flags |= _lib.BTC_BUILD_RADIX
+        if asynchronous:
+            flags |= _lib.BTC_BUILD_ASYNC
         check(lib().btc_rebuild_bitbsr(self._h, sp, dp, m, int(n), int(tile_cols), flags,
                                        _stream_ptr(stream)), "btc_rebuild_bitbsr")
-        del keep
+        self._keep = keep if asynchronous else None
 
     def count(self, tau: int = _lib.BTC_TAU_DEFAULT, stream=None, timing: bool = False):
         out = C.c_ulonglong(0)

@@ -366,10 +366,10 @@ static int batch_build_into(btc_batch* b, const int32_t* src, const int32_t* dst
                                                            g->prefix.as<uint32_t>(),
                                                            g->blocks.as<uint32_t>());
     }
-    BTC_TRY(g->rowmask.reserve(sizeof(uint32_t) * (tiles + 1)));
-    BTC_TRY(launch_rowmask(tile_cols, g->blocks.as<uint32_t>(), g->num_tiles,
+    BTC_TRY(g->rowmask.reserve(sizeof(uint32_t) * (tiles ? tiles : 1)));
+    BTC_TRY(launch_rowmask(tile_cols, g->blocks.as<uint32_t>(), g->num_tiles, nullptr,
                            g->indptr.as<uint32_t>(), g->n_row_blocks, g->rowmask.as<uint32_t>(),
-                           s));
+                           meta + kMetaRowMax, s));
     return cudaGetLastError() == cudaSuccess ? BTC_OK : BTC_E_CUDA;
 }
 
@@ -429,7 +429,7 @@ int btc_batch_count(btc_batch* b, int tau, btc_stream_t stream, unsigned long lo
                          g->row_indices.as<uint32_t>(), g->blocks.as<uint32_t>(), g->num_tiles,
                          g->n_row_blocks, tau, scr, stream, b->row_off.as<uint32_t>(),
                          (uint32_t)b->num_graphs, counts, g->rowmask.as<uint32_t>(), nullptr,
-                         nullptr, 0, g->rowmask.as<uint32_t>() + g->num_tiles));
+                         nullptr, 0, g->meta.as<unsigned long long>() + kMetaRowMax));
     if (h_counts) {
         BTC_CUDA_TRY(cudaMemcpyAsync(h_counts, counts, bytes, cudaMemcpyDeviceToHost, stream));
         BTC_CUDA_TRY(cudaStreamSynchronize(stream));

@@ -8,10 +8,11 @@
 //
 //   k_mark       one pass over the edges: orient (max,min), range-check, drop
 //                self-loops, set the cell bit (fire-and-forget atomicOr)
-//   k_bm_count   popcount per 4096-word chunk
-//   k_seg_scan   exclusive scan of the chunk counts -> chunk bases, tile total
+//   k_bm_count_scan  popcount per 4096-word chunk; the last CTA to finish scans the
+//                chunk counts into chunk bases and the tile total
 //   k_bm_emit    per word: exclusive tile prefix (kept for k_fill_bm), indices /
-//                row_indices of each set cell, indptr at row-block starts
+//                row_indices of each set cell, indptr at row-block starts; each CTA
+//                zeroes its chunk's tiles, the last one writes indptr[R]
 //   k_fill_bm    second pass over the edges: tile = prefix[word] + popc(lower bits of
 //                the word); OR the edge's bit into the tile
 //
@@ -125,13 +126,95 @@ k_bm_count(const uint32_t* __restrict__ bitmap, uint64_t W, uint32_t* __restrict
     }
 }
 
+// Chunk popcounts into chunk_base[b]; the last CTA to finish (a ticket in
+// meta[kMetaTicket], zeroed with the metadata) scans them in place into exclusive chunk
+// bases and writes the tile total to meta[kMetaTiles].  No CTA waits for another.
+__global__ void __launch_bounds__(kThreads)
+k_bm_count_scan(const uint32_t* __restrict__ bitmap, uint64_t W, uint32_t* chunk_base,
+                unsigned long long* meta)
+{
+    __shared__ uint32_t s_warp[kThreads / kWarp];
+    __shared__ unsigned long long s_tot[kThreads / kWarp];
+    __shared__ int s_last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t w0 = (uint64_t)blockIdx.x * kChunk + (uint64_t)threadIdx.x * kWordsPerThread;
+    uint32_t x[kWordsPerThread];
+    load16(bitmap, w0, W, x);
+    uint32_t sum = 0;
+#pragma unroll
+    for (int k = 0; k < kWordsPerThread; ++k) sum += __popc(x[k]);
+    sum = __reduce_add_sync(kFull, sum);
+    if (lane == 0) s_warp[warp] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < kThreads / kWarp; ++w) t += s_warp[w];
+        chunk_base[blockIdx.x] = t;
+        __threadfence();
+        s_last = atomicAdd(&meta[kMetaTicket], 1ull) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    // exclusive scan of the gridDim.x counts; thread t owns a contiguous run of them
+    const uint32_t nch = gridDim.x;
+    const uint32_t per = (nch + kThreads - 1) / kThreads;
+    const uint32_t b0 = min((uint32_t)threadIdx.x * per, nch), b1 = min(b0 + per, nch);
+    unsigned long long own = 0;
+    for (uint32_t b = b0; b < b1; ++b) own += __ldcg(&chunk_base[b]);
+    unsigned long long incl = own;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const unsigned long long t = __shfl_up_sync(kFull, incl, d);
+        if (lane >= d) incl += t;
+    }
+    if (lane == 31) s_tot[warp] = incl;
+    __syncthreads();
+    unsigned long long run = incl - own;
+    for (int w = 0; w < warp; ++w) run += s_tot[w];
+    for (uint32_t b = b0; b < b1; ++b) {
+        const uint32_t c = __ldcg(&chunk_base[b]);
+        chunk_base[b] = (uint32_t)run;
+        run += c;
+    }
+    if (threadIdx.x == kThreads - 1) meta[kMetaTiles] = run;  // the total
+}
+
+// indptr[R] = tile count; the overflow flag; and, when host_meta (a device alias of
+// mapped pinned memory) is given, the build's status slots copied to the host.
+__device__ __forceinline__ void finish_tiles(uint32_t* indptr, int32_t R, unsigned long long* meta,
+                                             uint32_t cap, unsigned long long* host_meta)
+{
+    const unsigned long long T = meta[kMetaTiles];
+    indptr[R] = (uint32_t)T;
+    if (T > cap) meta[kMetaOverflow] = 1ull;
+    if (host_meta) {
+        volatile unsigned long long* h = host_meta;
+        h[kMetaBad] = meta[kMetaBad];
+        h[kMetaTiles] = T;
+        h[kMetaOverflow] = T > cap ? 1ull : 0ull;
+        __threadfence_system();
+    }
+}
+
 __global__ void __launch_bounds__(kThreads)
 k_bm_emit(const uint32_t* __restrict__ bitmap, uint64_t W, uint64_t wpr,
           const uint32_t* __restrict__ chunk_base, uint32_t* __restrict__ prefix,
           uint32_t* __restrict__ indices, uint32_t* __restrict__ row_indices,
-          uint32_t* __restrict__ indptr)
+          uint32_t* __restrict__ indptr, unsigned long long* meta, uint32_t cap,
+          unsigned long long* host_meta, int32_t R, uint4* __restrict__ blocks, uint32_t tile_vec4)
 {
     __shared__ uint32_t s_warp[kThreads / kWarp];
+    const unsigned long long T = meta[kMetaTiles];
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) finish_tiles(indptr, R, meta, cap, host_meta);
+    if (T > cap) return;  // overflowed tile arrays: the builder redoes this step
+    {
+        // zero this chunk's tiles before k_fill_bm ORs bits into them
+        const uint64_t tb = chunk_base[blockIdx.x];
+        const uint64_t te = blockIdx.x + 1 < gridDim.x ? chunk_base[blockIdx.x + 1] : T;
+        for (uint64_t i = tb * tile_vec4 + threadIdx.x; i < te * tile_vec4; i += kThreads)
+            blocks[i] = make_uint4(0u, 0u, 0u, 0u);
+    }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t w0 = (uint64_t)blockIdx.x * kChunk + (uint64_t)threadIdx.x * kWordsPerThread;
     uint32_t x[kWordsPerThread];
@@ -193,8 +276,10 @@ template <int LOG2C>
 __global__ void __launch_bounds__(kThreads)
 k_fill_bm(const int32_t* __restrict__ src, const int32_t* __restrict__ dst, int64_t m, int32_t n,
           const int32_t* __restrict__ rank, uint64_t wpr, const uint32_t* __restrict__ bitmap,
-          const uint32_t* __restrict__ prefix, uint32_t* __restrict__ blocks)
+          const uint32_t* __restrict__ prefix, uint32_t* __restrict__ blocks,
+          const unsigned long long* __restrict__ d_tiles, uint32_t cap)
 {
+    if (*d_tiles > cap) return;  // overflowed tile arrays: the builder redoes this step
     constexpr int C = 1 << LOG2C;
     constexpr int WPR = C / 32;
     constexpr int TW = 16 * WPR;
@@ -234,10 +319,14 @@ k_fill_bm(const int32_t* __restrict__ src, const int32_t* __restrict__ dst, int6
     }
 }
 
+// indptr[R] = tile count; the overflow flag; and, when host_meta (a device alias of
+// mapped pinned memory) is given, the build's status slots copied to the host.
+// The same for a graph without cells (n = 0), where no k_bm_emit runs.
 __global__ void k_set_last(uint32_t* __restrict__ indptr, int32_t R,
-                           const unsigned long long* __restrict__ total)
+                           unsigned long long* __restrict__ meta, uint32_t cap,
+                           unsigned long long* __restrict__ host_meta)
 {
-    indptr[R] = (uint32_t)*total;
+    finish_tiles(indptr, R, meta, cap, host_meta);
 }
 
 template <int TW>
@@ -291,30 +380,35 @@ int bitmap_mark_and_count(const BuildGeom& g, const int32_t* src, const int32_t*
                                                                  meta_bad);
     }
     const size_t chunks = bitmap_chunks(W);
-    bm::k_bm_count<<<(unsigned)chunks, bm::kThreads, 0, s>>>(bitmap, W, chunk_count);
-    if (cudaGetLastError() != cudaSuccess) return BTC_E_CUDA;
-    return launch_tile_scan(chunk_count, (uint32_t)chunks, meta_tiles, s);
+    // meta_tiles - kMetaTiles is the metadata base (its ticket slot is zero)
+    bm::k_bm_count_scan<<<(unsigned)chunks, bm::kThreads, 0, s>>>(bitmap, W, chunk_count,
+                                                                   meta_tiles - kMetaTiles);
+    return cudaGetLastError() == cudaSuccess ? BTC_OK : BTC_E_CUDA;
 }
 
 int bitmap_emit_and_fill(const BuildGeom& g, const int32_t* src, const int32_t* dst, int64_t m,
                          const int32_t* rank, const uint32_t* bitmap, const uint32_t* chunk_base,
                          uint32_t* prefix, uint32_t* indices, uint32_t* row_indices,
-                         uint32_t* indptr, uint32_t* blocks, const unsigned long long* meta_tiles,
-                         cudaStream_t s)
+                         uint32_t* indptr, uint32_t* blocks, unsigned long long* meta,
+                         uint32_t cap, unsigned long long* host_meta, cudaStream_t s)
 {
+    const unsigned long long* meta_tiles = meta + kMetaTiles;
     const uint64_t wpr = bitmap_words_per_row(g);
     const uint64_t W = wpr * (uint64_t)g.n_row_blocks;
+    const uint32_t vec4 = 4u * (uint32_t)(g.tile_cols / 32);  // 16-byte words per tile
     if (W > 0)
         bm::k_bm_emit<<<(unsigned)bitmap_chunks(W), bm::kThreads, 0, s>>>(
-            bitmap, W, wpr, chunk_base, prefix, indices, row_indices, indptr);
-    bm::k_set_last<<<1, 1, 0, s>>>(indptr, g.n_row_blocks, meta_tiles);
+            bitmap, W, wpr, chunk_base, prefix, indices, row_indices, indptr, meta, cap,
+            host_meta, g.n_row_blocks, reinterpret_cast<uint4*>(blocks), vec4);
+    else
+        bm::k_set_last<<<1, 1, 0, s>>>(indptr, g.n_row_blocks, meta, cap, host_meta);
     if (m > 0 && W > 0) {
         if (g.tile_cols == 128)
-            bm::k_fill_bm<7><<<edge_grid(m), bm::kThreads, 0, s>>>(src, dst, m, g.n, rank, wpr,
-                                                                    bitmap, prefix, blocks);
+            bm::k_fill_bm<7><<<edge_grid(m), bm::kThreads, 0, s>>>(
+                src, dst, m, g.n, rank, wpr, bitmap, prefix, blocks, meta_tiles, cap);
         else
-            bm::k_fill_bm<5><<<edge_grid(m), bm::kThreads, 0, s>>>(src, dst, m, g.n, rank, wpr,
-                                                                    bitmap, prefix, blocks);
+            bm::k_fill_bm<5><<<edge_grid(m), bm::kThreads, 0, s>>>(
+                src, dst, m, g.n, rank, wpr, bitmap, prefix, blocks, meta_tiles, cap);
     }
     return cudaGetLastError() == cudaSuccess ? BTC_OK : BTC_E_CUDA;
 }
@@ -347,17 +441,21 @@ int launch_bitmap_count(const uint32_t* bitmap, uint64_t W, uint32_t* chunk_coun
 namespace btc200 {
 namespace bm {
 template <int WPR>
-__global__ void k_rowmask(const uint32_t* __restrict__ blocks, uint32_t num_tiles,
+__global__ void k_rowmask(const uint32_t* __restrict__ blocks, uint32_t cap,
+                          const unsigned long long* __restrict__ d_tiles,
                           const uint32_t* __restrict__ indptr, uint32_t R,
-                          uint32_t* __restrict__ rowmask)
+                          uint32_t* __restrict__ rowmask, unsigned long long* __restrict__ row_max)
 {
+    const unsigned long long T = d_tiles ? *d_tiles : cap;
+    if (T > cap) return;  // overflowed tile arrays: the builder redoes this step
+    const uint32_t num_tiles = (uint32_t)T;
     // longest row-block list
     uint32_t mx = 0;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < R;
          i += (uint64_t)gridDim.x * blockDim.x)
         mx = max(mx, indptr[i + 1] - indptr[i]);
     mx = __reduce_max_sync(kFull, mx);
-    if ((threadIdx.x & 31) == 0 && mx) atomicMax(rowmask + num_tiles, mx);
+    if ((threadIdx.x & 31) == 0 && mx) atomicMax(row_max, (unsigned long long)mx);
 
     for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < num_tiles;
          t += (uint64_t)gridDim.x * blockDim.x) {
@@ -384,19 +482,17 @@ __global__ void k_rowmask(const uint32_t* __restrict__ blocks, uint32_t num_tile
 }
 }  // namespace bm
 
-int launch_rowmask(int tile_cols, const uint32_t* blocks, uint32_t num_tiles,
-                   const uint32_t* indptr, int32_t n_row_blocks, uint32_t* rowmask,
-                   cudaStream_t s)
+int launch_rowmask(int tile_cols, const uint32_t* blocks, uint32_t cap,
+                   const unsigned long long* d_tiles, const uint32_t* indptr, int32_t n_row_blocks,
+                   uint32_t* rowmask, unsigned long long* row_max, cudaStream_t s)
 {
-    if (cudaMemsetAsync(rowmask + num_tiles, 0, sizeof(uint32_t), s) != cudaSuccess)
-        return BTC_E_CUDA;
     const uint32_t R = n_row_blocks > 0 ? (uint32_t)n_row_blocks : 0u;
-    if (num_tiles || R) {
-        const int grid = grid_for((int64_t)max(num_tiles, R), 256);
+    if (cap || R) {
+        const int grid = grid_for((int64_t)max(cap, R), 256);
         if (tile_cols == 128)
-            bm::k_rowmask<4><<<grid, 256, 0, s>>>(blocks, num_tiles, indptr, R, rowmask);
+            bm::k_rowmask<4><<<grid, 256, 0, s>>>(blocks, cap, d_tiles, indptr, R, rowmask, row_max);
         else
-            bm::k_rowmask<1><<<grid, 256, 0, s>>>(blocks, num_tiles, indptr, R, rowmask);
+            bm::k_rowmask<1><<<grid, 256, 0, s>>>(blocks, cap, d_tiles, indptr, R, rowmask, row_max);
     }
     return cudaGetLastError() == cudaSuccess ? BTC_OK : BTC_E_CUDA;
 }

@@ -10,6 +10,8 @@
 #include "common.cuh"
 #include "handle.cuh"
 
+#include <algorithm>
+
 namespace btc200 {
 
 int launch_degree(const int32_t*, const int32_t*, int64_t, int32_t, uint32_t*, cudaStream_t);
@@ -27,7 +29,8 @@ int bitmap_mark_and_count(const BuildGeom&, const int32_t*, const int32_t*, int6
                           uint32_t*, uint32_t*, unsigned long long*, unsigned long long*, cudaStream_t);
 int bitmap_emit_and_fill(const BuildGeom&, const int32_t*, const int32_t*, int64_t, const int32_t*,
                          const uint32_t*, const uint32_t*, uint32_t*, uint32_t*, uint32_t*, uint32_t*,
-                         uint32_t*, const unsigned long long*, cudaStream_t);
+                         uint32_t*, unsigned long long*, uint32_t, unsigned long long*,
+                         cudaStream_t);
 int launch_popcount_sum(int, const uint32_t*, uint64_t, unsigned long long*, cudaStream_t);
 int launch_indptr(const uint32_t*, uint32_t, int32_t, uint32_t*, cudaStream_t);
 int launch_density(int, const uint32_t*, uint32_t, unsigned long long*, cudaStream_t);
@@ -82,82 +85,70 @@ int ensure_count_scratch(btc_bitbsr* g)
     return BTC_OK;
 }
 
-static int build_into(btc_bitbsr* g, const int32_t* src, const int32_t* dst, int64_t m, int32_t n,
-                      int tile_cols, uint32_t flags, cudaStream_t s)
+// Pinned host slots the device writes directly (mapped): build status, tile count and
+// the count result reach the host without a copy-engine hop.
+int ensure_host_meta(btc_bitbsr* g)
 {
-    if (n < 0 || m < 0 || (uint64_t)m > kMaxEdges) return BTC_E_INVAL;
-    if (m > 0 && (!src || !dst)) return BTC_E_INVAL;
-    if (flags & ~(BTC_INPUT_ON_HOST | BTC_ORIENT_DEGREE | BTC_BUILD_RADIX)) return BTC_E_INVAL;
-    if (tile_cols == 0) tile_cols = btc_lite_select_tile_cols(m, n, 0);
-    if (tile_cols != 32 && tile_cols != 128) return BTC_E_INVAL;
-    BTC_CUDA_TRY(cudaGetDevice(&g->device));
-
-    const BuildGeom geom = make_geom(n, tile_cols);
-    g->tile_cols = tile_cols;
-    g->n = n;
-    g->n_row_blocks = geom.n_row_blocks;
-    g->input_edges = m;
-    g->edges_known = false;
-    g->num_edges = 0;
-
-    if (!g->h_meta) {
-        void* p = nullptr;
-        if (cudaMallocHost(&p, sizeof(unsigned long long) * kMetaSlots) != cudaSuccess) {
-            cudaGetLastError();
-            return BTC_E_NOMEM;
-        }
-        g->h_meta = static_cast<unsigned long long*>(p);
+    if (g->h_meta) return BTC_OK;
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, sizeof(unsigned long long) * kMetaSlots,
+                      cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess) {
+        cudaGetLastError();
+        return BTC_E_NOMEM;
     }
-    BTC_TRY(g->meta.reserve(sizeof(unsigned long long) * kMetaSlots));
+    void* d = nullptr;
+    if (cudaHostGetDevicePointer(&d, p, 0) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFreeHost(p);
+        return BTC_E_CUDA;
+    }
+    std::memset(p, 0, sizeof(unsigned long long) * kMetaSlots);
+    g->h_meta = static_cast<unsigned long long*>(p);
+    g->d_hmeta = static_cast<unsigned long long*>(d);
+    return BTC_OK;
+}
+
+// What one build enqueues, fixed before anything is enqueued (every buffer reserved).
+struct BuildPlan {
+    BuildGeom geom;
+    const int32_t* src;  // caller's arrays (host with BTC_INPUT_ON_HOST)
+    const int32_t* dst;
+    const int32_t* d_src;  // device arrays the kernels read
+    const int32_t* d_dst;
+    int64_t m;
+    int32_t n;
+    uint32_t flags;
+    bool use_bitmap;
+    bool degree;
+    uint64_t bm_words;
+    uint32_t cap;  // > 0: the post-count steps run against this tile capacity
+};
+
+// Enqueues the build up to the tile count (bitmap path) or up to the tile segmentation
+// (radix path), and with plan.cap > 0 the whole bitmap build.  No waits, no allocation:
+// this sequence is what a cached CUDA graph replays.
+static int enqueue_build(btc_bitbsr* g, const BuildPlan& P, uint64_t** sorted_out, cudaStream_t s)
+{
+    const BuildGeom& geom = P.geom;
     unsigned long long* meta = g->meta.as<unsigned long long>();
     BTC_CUDA_TRY(cudaMemsetAsync(meta, 0, sizeof(unsigned long long) * kMetaSlots, s));
-
-    // ---- input --------------------------------------------------------------
-    const int32_t* d_src = src;
-    const int32_t* d_dst = dst;
-    if ((flags & BTC_INPUT_ON_HOST) && m > 0) {
-        BTC_TRY(g->in_src.reserve(sizeof(int32_t) * (size_t)m));
-        BTC_TRY(g->in_dst.reserve(sizeof(int32_t) * (size_t)m));
-        BTC_CUDA_TRY(cudaMemcpyAsync(g->in_src.ptr, src, sizeof(int32_t) * (size_t)m,
+    if ((P.flags & BTC_INPUT_ON_HOST) && P.m > 0) {
+        BTC_CUDA_TRY(cudaMemcpyAsync(g->in_src.ptr, P.src, sizeof(int32_t) * (size_t)P.m,
                                      cudaMemcpyHostToDevice, s));
-        BTC_CUDA_TRY(cudaMemcpyAsync(g->in_dst.ptr, dst, sizeof(int32_t) * (size_t)m,
+        BTC_CUDA_TRY(cudaMemcpyAsync(g->in_dst.ptr, P.dst, sizeof(int32_t) * (size_t)P.m,
                                      cudaMemcpyHostToDevice, s));
-        d_src = g->in_src.as<int32_t>();
-        d_dst = g->in_dst.as<int32_t>();
     }
-
-    // The cell bitmap (one bit per (row block, column block)) replaces the sort when it
-    // is small next to the edge list; otherwise the radix path sorts tile keys.
-    const uint64_t wpr = bitmap_words_per_row(geom);
-    const uint64_t bm_words = wpr * (uint64_t)geom.n_row_blocks;
-    const uint64_t bm_bytes = 4 * bm_words;
-    const bool use_bitmap = !(flags & BTC_BUILD_RADIX) && bm_bytes <= (4ull << 30) &&
-                            bm_bytes <= 32ull * (uint64_t)m + (64ull << 20);
-    g->used_bitmap = use_bitmap;
-
-    const bool degree = (flags & BTC_ORIENT_DEGREE) && n > 0;
-    size_t key_cap = use_bitmap ? 0 : (size_t)m;
-    if (degree && (size_t)n > key_cap) key_cap = (size_t)n;
-    if (key_cap) {
-        BTC_TRY(g->keys0.reserve(sizeof(uint64_t) * key_cap));
-        BTC_TRY(g->keys1.reserve(sizeof(uint64_t) * key_cap));
-        BTC_TRY(g->sort_scratch.reserve(sizeof(uint32_t) * radix_scratch_words(key_cap)));
-    }
-    const size_t chunk_slots =
-        use_bitmap ? bitmap_chunks(bm_words) : sort_tiles((size_t)m);
-    BTC_TRY(g->tile_base.reserve(sizeof(uint32_t) * (chunk_slots + 1)));
     uint64_t* k0 = g->keys0.as<uint64_t>();
     uint64_t* k1 = g->keys1.as<uint64_t>();
     int st = BTC_OK;
 
     // ---- optional descending-degree relabel ---------------------------------
     const int32_t* rank = nullptr;
-    if (degree) {
-        BTC_TRY(g->deg.reserve(sizeof(uint32_t) * (size_t)n));
-        BTC_TRY(g->rank.reserve(sizeof(int32_t) * (size_t)n));
+    if (P.degree) {
+        const int32_t n = P.n;
         BTC_CUDA_TRY(cudaMemsetAsync(g->deg.ptr, 0, sizeof(uint32_t) * (size_t)n, s));
-        BTC_TRY(launch_degree(d_src, d_dst, m, n, g->deg.as<uint32_t>(), s));
-        int db = bit_length_u64(2ull * (uint64_t)m);  // degrees fit in db bits
+        BTC_TRY(launch_degree(P.d_src, P.d_dst, P.m, n, g->deg.as<uint32_t>(), s));
+        int db = bit_length_u64(2ull * (uint64_t)P.m);  // degrees fit in db bits
         if (db > 32) db = 32;
         const uint32_t dmax = db >= 32 ? 0xffffffffu : ((1u << db) - 1u);
         BTC_TRY(launch_rank_keys(g->deg.as<uint32_t>(), n, dmax, k0, s));
@@ -169,23 +160,193 @@ static int build_into(btc_bitbsr* g, const int32_t* src, const int32_t* dst, int
         rank = g->rank.as<int32_t>();
     }
 
-    const size_t TW = (size_t)16 * (tile_cols / 32);
-    uint64_t* sorted = nullptr;
-    if (use_bitmap) {
-        BTC_TRY(g->bitmap.reserve(sizeof(uint32_t) * (bm_words ? bm_words : 1)));
-        BTC_TRY(g->prefix.reserve(sizeof(uint32_t) * (bm_words ? bm_words : 1)));
-        BTC_TRY(bitmap_mark_and_count(geom, d_src, d_dst, m, rank, g->bitmap.as<uint32_t>(),
+    if (P.use_bitmap) {
+        BTC_TRY(bitmap_mark_and_count(geom, P.d_src, P.d_dst, P.m, rank, g->bitmap.as<uint32_t>(),
                                       g->tile_base.as<uint32_t>(), meta + kMetaBad,
                                       meta + kMetaTiles, s));
+        if (P.cap) {
+            BTC_TRY(bitmap_emit_and_fill(geom, P.d_src, P.d_dst, P.m, rank,
+                                         g->bitmap.as<uint32_t>(), g->tile_base.as<uint32_t>(),
+                                         g->prefix.as<uint32_t>(), g->indices.as<uint32_t>(),
+                                         g->row_indices.as<uint32_t>(), g->indptr.as<uint32_t>(),
+                                         g->blocks.as<uint32_t>(), meta, P.cap, g->d_hmeta, s));
+            BTC_TRY(launch_rowmask(geom.tile_cols, g->blocks.as<uint32_t>(), P.cap,
+                                   meta + kMetaTiles, g->indptr.as<uint32_t>(), geom.n_row_blocks,
+                                   g->rowmask.as<uint32_t>(), meta + kMetaRowMax, s));
+        }
     } else {
         // ---- keys, sort, segmentation ---------------------------------------
-        BTC_TRY(launch_make_keys(geom, d_src, d_dst, m, rank, k0, meta, s));
-        sorted = radix_sort_u64(k0, k1, (size_t)m, meta + kMetaValid, geom.payload_bits,
-                                geom.payload_bits + geom.t_bits, g->sort_scratch.as<uint32_t>(), s,
-                                &st);
+        BTC_TRY(launch_make_keys(geom, P.d_src, P.d_dst, P.m, rank, k0, meta, s));
+        uint64_t* sorted = radix_sort_u64(k0, k1, (size_t)P.m, meta + kMetaValid,
+                                          geom.payload_bits, geom.payload_bits + geom.t_bits,
+                                          g->sort_scratch.as<uint32_t>(), s, &st);
         BTC_TRY(st);
-        BTC_TRY(launch_segment(geom, sorted, (size_t)m, meta + kMetaValid,
+        BTC_TRY(launch_segment(geom, sorted, (size_t)P.m, meta + kMetaValid,
                                g->tile_base.as<uint32_t>(), meta + kMetaTiles, s));
+        *sorted_out = sorted;
+    }
+    return BTC_OK;
+}
+
+// Everything an enqueued build reads or writes, plus its arguments: a graph captured
+// from enqueue_build replays only under the same key.
+static void build_key(const btc_bitbsr* g, const BuildPlan& P, BuildGraphKey* k)
+{
+    std::memset(k, 0, sizeof(*k));
+    const void* w[] = {P.src, P.dst, g->meta.ptr, g->in_src.ptr, g->in_dst.ptr, g->keys0.ptr,
+                       g->keys1.ptr, g->sort_scratch.ptr, g->deg.ptr, g->rank.ptr, g->bitmap.ptr,
+                       g->prefix.ptr, g->tile_base.ptr, g->indices.ptr, g->row_indices.ptr,
+                       g->indptr.ptr, g->blocks.ptr, g->rowmask.ptr, g->d_hmeta};
+    static_assert(sizeof(w) / sizeof(w[0]) == kBuildKeyPtrs, "key layout");
+    for (int i = 0; i < kBuildKeyPtrs; ++i) k->ptr[i] = w[i];
+    k->m = P.m;
+    k->n = P.n;
+    k->tile_cols = P.geom.tile_cols;
+    k->flags = P.flags;
+    k->cap = P.cap;
+}
+
+// Replays (or, on the second identical call, captures) the enqueued build as a CUDA
+// graph: one launch instead of about a dozen.  Returns false when it did not enqueue.
+static bool launch_build_graph(btc_bitbsr* g, const BuildPlan& P, cudaStream_t s)
+{
+    BuildGraphKey key;
+    build_key(g, P, &key);
+    if (g->graph_exec && std::memcmp(&key, &g->graph_key, sizeof(key)) == 0)
+        return cudaGraphLaunch(g->graph_exec, s) == cudaSuccess;
+    const bool repeat = std::memcmp(&key, &g->last_key, sizeof(key)) == 0;
+    g->last_key = key;
+    if (!repeat) return false;
+    if (!g->capture_stream &&
+        cudaStreamCreateWithFlags(&g->capture_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(g->capture_stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    uint64_t* unused = nullptr;
+    const int st = enqueue_build(g, P, &unused, g->capture_stream);
+    const cudaError_t e = cudaStreamEndCapture(g->capture_stream, &graph);
+    cudaGraphExec_t exec = nullptr;
+    const bool ok = st == BTC_OK && e == cudaSuccess && graph &&
+                    cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
+    if (!ok) {
+        cudaGetLastError();
+        if (exec) cudaGraphExecDestroy(exec);
+        return false;
+    }
+    if (g->graph_exec) cudaGraphExecDestroy(g->graph_exec);
+    g->graph_exec = exec;
+    g->graph_key = key;
+    return cudaGraphLaunch(g->graph_exec, s) == cudaSuccess;
+}
+
+static int build_into(btc_bitbsr* g, const int32_t* src, const int32_t* dst, int64_t m, int32_t n,
+                      int tile_cols, uint32_t flags, cudaStream_t s)
+{
+    if (n < 0 || m < 0 || (uint64_t)m > kMaxEdges) return BTC_E_INVAL;
+    if (m > 0 && (!src || !dst)) return BTC_E_INVAL;
+    if (flags & ~(BTC_INPUT_ON_HOST | BTC_ORIENT_DEGREE | BTC_BUILD_RADIX | BTC_BUILD_ASYNC))
+        return BTC_E_INVAL;
+    if (g->pending) resolve_build(g);  // an enqueued build still owns the buffers
+    if (tile_cols == 0) tile_cols = btc_lite_select_tile_cols(m, n, 0);
+    if (tile_cols != 32 && tile_cols != 128) return BTC_E_INVAL;
+    BTC_CUDA_TRY(cudaGetDevice(&g->device));
+
+    BuildPlan P{};
+    P.geom = make_geom(n, tile_cols);
+    const BuildGeom& geom = P.geom;
+    g->tile_cols = tile_cols;
+    g->n = n;
+    g->n_row_blocks = geom.n_row_blocks;
+    g->input_edges = m;
+    g->edges_known = false;
+    g->num_edges = 0;
+
+    // ---- reserve every buffer the enqueued steps use ---------------------------
+    BTC_TRY(ensure_host_meta(g));
+    BTC_TRY(g->meta.reserve(sizeof(unsigned long long) * kMetaSlots));
+    unsigned long long* meta = g->meta.as<unsigned long long>();
+    P.src = src;
+    P.dst = dst;
+    P.d_src = src;
+    P.d_dst = dst;
+    P.m = m;
+    P.n = n;
+    P.flags = flags;
+    if ((flags & BTC_INPUT_ON_HOST) && m > 0) {
+        BTC_TRY(g->in_src.reserve(sizeof(int32_t) * (size_t)m));
+        BTC_TRY(g->in_dst.reserve(sizeof(int32_t) * (size_t)m));
+        P.d_src = g->in_src.as<int32_t>();
+        P.d_dst = g->in_dst.as<int32_t>();
+    }
+    // The cell bitmap (one bit per (row block, column block)) replaces the sort when it
+    // is small next to the edge list; otherwise the radix path sorts tile keys.
+    const uint64_t wpr = bitmap_words_per_row(geom);
+    P.bm_words = wpr * (uint64_t)geom.n_row_blocks;
+    const uint64_t bm_bytes = 4 * P.bm_words;
+    P.use_bitmap = !(flags & BTC_BUILD_RADIX) && bm_bytes <= (4ull << 30) &&
+                   bm_bytes <= 32ull * (uint64_t)m + (64ull << 20);
+    g->used_bitmap = P.use_bitmap;
+    P.degree = (flags & BTC_ORIENT_DEGREE) && n > 0;
+    size_t key_cap = P.use_bitmap ? 0 : (size_t)m;
+    if (P.degree && (size_t)n > key_cap) key_cap = (size_t)n;
+    if (key_cap) {
+        BTC_TRY(g->keys0.reserve(sizeof(uint64_t) * key_cap));
+        BTC_TRY(g->keys1.reserve(sizeof(uint64_t) * key_cap));
+        BTC_TRY(g->sort_scratch.reserve(sizeof(uint32_t) * radix_scratch_words(key_cap)));
+    }
+    const size_t chunk_slots = P.use_bitmap ? bitmap_chunks(P.bm_words) : sort_tiles((size_t)m);
+    BTC_TRY(g->tile_base.reserve(sizeof(uint32_t) * (chunk_slots + 1)));
+    if (P.degree) {
+        BTC_TRY(g->deg.reserve(sizeof(uint32_t) * (size_t)n));
+        BTC_TRY(g->rank.reserve(sizeof(int32_t) * (size_t)n));
+    }
+    if (P.use_bitmap) {
+        BTC_TRY(g->bitmap.reserve(sizeof(uint32_t) * (P.bm_words ? P.bm_words : 1)));
+        BTC_TRY(g->prefix.reserve(sizeof(uint32_t) * (P.bm_words ? P.bm_words : 1)));
+    }
+    BTC_TRY(g->indptr.reserve(sizeof(uint32_t) * ((size_t)geom.n_row_blocks + 1)));
+    BTC_TRY(ensure_count_scratch(g));
+
+    const size_t TW = (size_t)16 * (tile_cols / 32);
+    // Tiles the arrays already hold room for (a rebuild): the bitmap path then enqueues
+    // the whole build against that capacity, with every post-count kernel checking the
+    // device tile count, and waits once at the end (or not at all with BTC_BUILD_ASYNC);
+    // a count above the capacity is redone below at the right size.  A first build
+    // waits for the count in between.
+    if (P.use_bitmap && g->indices.ptr && g->row_indices.ptr && g->blocks.ptr && g->rowmask.ptr) {
+        uint64_t c = g->indices.bytes / 4;
+        c = std::min<uint64_t>(c, g->row_indices.bytes / 4);
+        c = std::min<uint64_t>(c, g->blocks.bytes / (4 * TW));
+        c = std::min<uint64_t>(c, g->rowmask.bytes / 4);
+        P.cap = (uint32_t)std::min<uint64_t>(c, 0xffffffffull);
+    }
+
+    uint64_t* sorted = nullptr;
+    if (P.cap) {
+        // repeated identical asynchronous rebuilds of device input replay a CUDA graph
+        const bool graphed = (flags & BTC_BUILD_ASYNC) && !(flags & BTC_INPUT_ON_HOST) &&
+                             launch_build_graph(g, P, s);
+        if (!graphed) BTC_TRY(enqueue_build(g, P, &sorted, s));
+        // the build's status and tile count are in h_meta once the stream has run it
+        // (k_set_last writes them through the mapping)
+        if (!g->meta_event)
+            BTC_CUDA_TRY(cudaEventCreateWithFlags(&g->meta_event, cudaEventDisableTiming));
+        BTC_CUDA_TRY(cudaEventRecord(g->meta_event, s));
+        g->pending = true;
+        g->pending_cap = P.cap;
+        if (flags & BTC_BUILD_ASYNC) return BTC_OK;  // resolved by the next wait
+        const int st2 = resolve_build(g);
+        if (st2 != BTC_E_CAPACITY) return st2;
+        // more tiles than the arrays hold: redo the post-count steps at the right size
+        BTC_CUDA_TRY(cudaMemsetAsync(meta + kMetaOverflow, 0, sizeof(unsigned long long), s));
+    } else {
+        BTC_TRY(enqueue_build(g, P, &sorted, s));
     }
     BTC_CUDA_TRY(cudaMemcpyAsync(g->h_meta, meta, sizeof(unsigned long long) * 3,
                                  cudaMemcpyDeviceToHost, s));
@@ -196,51 +357,78 @@ static int build_into(btc_bitbsr* g, const int32_t* src, const int32_t* dst, int
     g->num_tiles = (uint32_t)tiles;
 
     // ---- tile arrays ----------------------------------------------------------
-    BTC_TRY(g->indptr.reserve(sizeof(uint32_t) * ((size_t)geom.n_row_blocks + 1)));
     BTC_TRY(g->indices.reserve(sizeof(uint32_t) * (tiles ? tiles : 1)));
     BTC_TRY(g->row_indices.reserve(sizeof(uint32_t) * (tiles ? tiles : 1)));
     BTC_TRY(g->blocks.reserve(sizeof(uint32_t) * TW * (tiles ? tiles : 1)));
-    BTC_TRY(ensure_count_scratch(g));
-    if (tiles)
-        BTC_CUDA_TRY(cudaMemsetAsync(g->blocks.ptr, 0, sizeof(uint32_t) * TW * tiles, s));
-    if (use_bitmap) {
-        BTC_TRY(bitmap_emit_and_fill(geom, d_src, d_dst, m, rank, g->bitmap.as<uint32_t>(),
-                                     g->tile_base.as<uint32_t>(), g->prefix.as<uint32_t>(),
-                                     g->indices.as<uint32_t>(), g->row_indices.as<uint32_t>(),
-                                     g->indptr.as<uint32_t>(), g->blocks.as<uint32_t>(),
-                                     meta + kMetaTiles, s));
+    if (P.use_bitmap) {
+        BTC_TRY(bitmap_emit_and_fill(geom, P.d_src, P.d_dst, m, P.degree ? g->rank.as<int32_t>() : nullptr,
+                                     g->bitmap.as<uint32_t>(), g->tile_base.as<uint32_t>(),
+                                     g->prefix.as<uint32_t>(), g->indices.as<uint32_t>(),
+                                     g->row_indices.as<uint32_t>(), g->indptr.as<uint32_t>(),
+                                     g->blocks.as<uint32_t>(), meta, (uint32_t)tiles, nullptr, s));
     } else {
+        if (tiles)
+            BTC_CUDA_TRY(cudaMemsetAsync(g->blocks.ptr, 0, sizeof(uint32_t) * TW * tiles, s));
         BTC_TRY(launch_fill(geom, sorted, (size_t)m, meta + kMetaValid, g->tile_base.as<uint32_t>(),
                             g->indices.as<uint32_t>(), g->row_indices.as<uint32_t>(),
                             g->blocks.as<uint32_t>(), s));
         BTC_TRY(launch_indptr(g->row_indices.as<uint32_t>(), g->num_tiles, geom.n_row_blocks,
                               g->indptr.as<uint32_t>(), s));
     }
-    BTC_TRY(g->rowmask.reserve(sizeof(uint32_t) * (tiles + 1)));
-    BTC_TRY(launch_rowmask(tile_cols, g->blocks.as<uint32_t>(), g->num_tiles,
+    BTC_TRY(g->rowmask.reserve(sizeof(uint32_t) * (tiles ? tiles : 1)));
+    BTC_TRY(launch_rowmask(tile_cols, g->blocks.as<uint32_t>(), g->num_tiles, nullptr,
                            g->indptr.as<uint32_t>(), g->n_row_blocks, g->rowmask.as<uint32_t>(),
-                           s));
+                           meta + kMetaRowMax, s));
     return BTC_OK;
 }
 
 int count_handle(btc_bitbsr* g, int tau, cudaStream_t s, unsigned long long* d_out2,
-                 uint32_t tile_begin, uint32_t tile_end)
+                 uint32_t tile_begin, uint32_t tile_end, bool to_host)
 {
     if (!g) return BTC_E_INVAL;
     if (tau == BTC_TAU_DEFAULT) tau = default_tau(g->tile_cols);
     if (tau < 0) return BTC_E_INVAL;
+    if (!g->pending && g->failed != BTC_OK) return g->failed;
     BTC_TRY(ensure_count_scratch(g));
     CountScratch scr{g->partials.as<unsigned long long>(), g->done.as<unsigned int>(),
                      reinterpret_cast<unsigned long long*>(g->done.as<char>() + 8),
                      g->result.as<unsigned long long>(), d_out2};
+    if (to_host) {
+        BTC_TRY(ensure_host_meta(g));
+        scr.result_host = g->d_hmeta + 7;
+    }
+    // after an enqueued build the kernel reads the tile count (and the build's status)
+    // from the device; the capacity bounds it
+    const unsigned long long* build_meta = g->pending ? g->meta.as<unsigned long long>() : nullptr;
     return launch_count(g->tile_cols, g->indptr.as<uint32_t>(), g->indices.as<uint32_t>(),
-                        g->row_indices.as<uint32_t>(), g->blocks.as<uint32_t>(), g->num_tiles,
-                        g->n_row_blocks, tau, scr, s, nullptr, 0, nullptr,
-                        g->rowmask.as<uint32_t>(),
+                        g->row_indices.as<uint32_t>(), g->blocks.as<uint32_t>(),
+                        g->pending ? g->pending_cap : g->num_tiles, g->n_row_blocks, tau, scr, s,
+                        nullptr, 0, nullptr, g->rowmask.as<uint32_t>(),
                         g->used_bitmap ? g->bitmap.as<uint32_t>() : nullptr,
                         g->used_bitmap ? g->prefix.as<uint32_t>() : nullptr,
                         bitmap_words_per_row(make_geom(g->n, g->tile_cols)),
-                        g->rowmask.as<uint32_t>() + g->num_tiles, tile_begin, tile_end);
+                        g->meta.as<unsigned long long>() + kMetaRowMax, tile_begin, tile_end,
+                        build_meta, g->num_tiles);
+}
+
+int resolve_build(btc_bitbsr* g)
+{
+    if (!g->pending) return g->failed;
+    g->pending = false;
+    if (cudaEventSynchronize(g->meta_event) != cudaSuccess) {
+        cudaGetLastError();
+        return g->failed = BTC_E_CUDA;
+    }
+    const unsigned long long* h = g->h_meta;
+    if (h[kMetaBad] != 0) {
+        g->failed = BTC_E_RANGE;
+    } else if (h[kMetaOverflow] != 0 || h[kMetaTiles] > g->pending_cap) {
+        g->failed = BTC_E_CAPACITY;
+    } else {
+        g->num_tiles = (uint32_t)h[kMetaTiles];
+        g->failed = BTC_OK;
+    }
+    return g->failed;
 }
 
 // ===========================================================================
@@ -261,6 +449,7 @@ const char* btc_strerror(int status)
     case BTC_E_CUDA: return "CUDA error";
     case BTC_E_TIMEOUT: return "device wait timed out";
     case BTC_E_RANGE: return "vertex id out of range";
+    case BTC_E_CAPACITY: return "an enqueued rebuild needed more tiles than the handle held";
     default: return "unknown status";
     }
 }
@@ -294,7 +483,9 @@ int btc_rebuild_bitbsr(btc_bitbsr* g, const int32_t* src, const int32_t* dst, in
                        int tile_cols, uint32_t flags, btc_stream_t stream)
 {
     if (!g) return BTC_E_INVAL;
-    return build_into(g, src, dst, m, n, tile_cols, flags, stream);
+    const int st = build_into(g, src, dst, m, n, tile_cols, flags, stream);
+    if (!g->pending) g->failed = st;  // an enqueued build's status comes with resolve_build
+    return st;
 }
 
 int btc_count_async(btc_bitbsr* g, int tau, btc_stream_t stream, unsigned long long* d_out)
@@ -312,13 +503,11 @@ int btc_count(btc_bitbsr* g, int tau, btc_stream_t stream, unsigned long long* o
         BTC_CUDA_TRY(cudaEventCreate(&e1));
         BTC_CUDA_TRY(cudaEventRecord(e0, stream));
     }
-    int st = count_handle(g, tau, stream, nullptr);
+    // the count kernel's last CTA writes the result into h_meta[7] through the mapping
+    int st = count_handle(g, tau, stream, nullptr, 0, 0xffffffffu, true);
     if (st == BTC_OK && kernel_ms && cudaEventRecord(e1, stream) != cudaSuccess) st = BTC_E_CUDA;
-    if (st == BTC_OK &&
-        cudaMemcpyAsync(g->h_meta + 7, g->result.ptr, sizeof(unsigned long long),
-                        cudaMemcpyDeviceToHost, stream) != cudaSuccess)
-        st = BTC_E_CUDA;
     if (st == BTC_OK && cudaStreamSynchronize(stream) != cudaSuccess) st = BTC_E_CUDA;
+    if (st == BTC_OK) st = resolve_build(g);
     if (st == BTC_OK) {
         *out_count = g->h_meta[7];
         if (kernel_ms) cudaEventElapsedTime(kernel_ms, e0, e1);
@@ -332,6 +521,7 @@ int btc_bitbsr_info(const btc_bitbsr* gc, btc_bitbsr_view* v)
 {
     if (!gc || !v) return BTC_E_INVAL;
     btc_bitbsr* g = const_cast<btc_bitbsr*>(gc);
+    BTC_TRY(resolve_build(g));
     if (!g->edges_known) {
         // unique lower edges = bits set in the tiles (duplicates OR the same bit); the
         // build may have run on any stream, so wait for the device first
@@ -363,6 +553,7 @@ int btc_bitbsr_info(const btc_bitbsr* gc, btc_bitbsr_view* v)
 int btc_density_hist(btc_bitbsr* g, btc_stream_t stream, uint64_t* hist)
 {
     if (!g || !hist) return BTC_E_INVAL;
+    BTC_TRY(resolve_build(g));
     const size_t nb = (size_t)16 * g->tile_cols + 1;
     DevBuf d;
     BTC_TRY(d.reserve(sizeof(unsigned long long) * nb));

@@ -140,6 +140,9 @@ struct CountScratch {
     unsigned long long* work;      // tile queue head (reset to 0 by the last CTA)
     unsigned long long* result;    // where the final count lands
     unsigned long long* result2;   // optional second destination (nullable)
+    // optional device alias of mapped pinned host memory that also receives the count
+    // (written by the last CTA, no copy-engine hop)
+    unsigned long long* result_host = nullptr;
 };
 
 int count_grid_size(int tile_cols);
@@ -152,15 +155,32 @@ int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
                  const uint32_t* graph_rows = nullptr, uint32_t num_graphs = 0,
                  unsigned long long* graph_counts = nullptr, const uint32_t* rowmask = nullptr,
                  const uint32_t* cellbm = nullptr, const uint32_t* cellpre = nullptr,
-                 uint64_t cell_wpr = 0, const uint32_t* row_max = nullptr,
-                 uint32_t tile_begin = 0, uint32_t tile_end = 0xffffffffu);
+                 uint64_t cell_wpr = 0, const unsigned long long* row_max = nullptr,
+                 uint32_t tile_begin = 0, uint32_t tile_end = 0xffffffffu,
+                 const unsigned long long* build_meta = nullptr, uint32_t tiles_hint = 0);
 
-// rowmask[t] bit r = tile t's row r has a bit (built after the tiles are filled), and
-// rowmask[num_tiles] = the most tiles in one row block (indptr's largest step), which
-// picks the count kernel's schedule.  rowmask holds num_tiles + 1 words.
-int launch_rowmask(int tile_cols, const uint32_t* blocks, uint32_t num_tiles,
-                   const uint32_t* indptr, int32_t n_row_blocks, uint32_t* rowmask,
-                   cudaStream_t s);
+// rowmask[t] bit r = tile t's row r has a bit, for t < T = *d_tiles (T = cap when d_tiles
+// is null), and *row_max = max(*row_max, the most tiles in one row block), which picks
+// the count kernel's schedule (the caller zeroes it).  Runs after the tiles are filled.
+// Writes nothing when T > cap (the tile arrays overflowed).
+int launch_rowmask(int tile_cols, const uint32_t* blocks, uint32_t cap,
+                   const unsigned long long* d_tiles, const uint32_t* indptr, int32_t n_row_blocks,
+                   uint32_t* rowmask, unsigned long long* row_max, cudaStream_t s);
+
+// Device metadata slots of a build (uint64 each): valid keys, out-of-range flag, tile
+// count, unique edges, sort length, longest row-block list, tile-capacity overflow flag,
+// and the chunk-scan ticket (CTAs of the chunk popcount that have finished).
+enum {
+    kMetaValid = 0,
+    kMetaBad = 1,
+    kMetaTiles = 2,
+    kMetaUniq = 3,
+    kMetaN = 4,
+    kMetaRowMax = 5,
+    kMetaOverflow = 6,
+    kMetaTicket = 7,
+    kMetaSlots = 8
+};
 
 // Queue/completion words of the count kernel: done (u32) at byte 0, work (u64) at 8.
 constexpr size_t kCountCtlBytes = 16;

@@ -40,6 +40,8 @@
 //    pack four matches into the 128-bit k dimension, as tc_16x32_mma_v6.h:72-154 does.
 #include "common.cuh"
 
+#include <atomic>
+
 namespace btc200 {
 
 namespace {
@@ -337,7 +339,8 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
         const uint32_t* __restrict__ graph_rows, uint32_t num_graphs,
         unsigned long long* __restrict__ graph_counts, const uint32_t* __restrict__ rowmask,
         const uint32_t* __restrict__ cellbm, const uint32_t* __restrict__ cellpre, uint64_t cell_wpr,
-        uint32_t chunk_skewed, const uint32_t* __restrict__ row_max)
+        uint32_t chunk_skewed, const unsigned long long* __restrict__ row_max,
+        const unsigned long long* __restrict__ build_meta)
 {
     using K = Cfg<C>;
     constexpr int WPR = K::WPR, TW = K::TW, JPT = K::JPT;
@@ -349,6 +352,18 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
     WarpSmem<C>& s = smem_all[warp];
     const unsigned lt = lanemask_lt();
     const int g = lane >> 2, tg = lane & 3;  // mma fragment coordinates
+
+    // A build enqueued without waiting (build_meta != nullptr): the tile count comes from
+    // the device, and a failed build (bad vertex id, tile capacity overflow) counts
+    // nothing and leaves 0xFFFFFFFFFFFFFFFF as the result.
+    bool build_failed = false;
+    if (build_meta) {
+        const unsigned long long T = build_meta[kMetaTiles];
+        build_failed = (build_meta[kMetaBad] | build_meta[kMetaOverflow]) != 0ull;
+        num_tiles = T < num_tiles ? (uint32_t)T : num_tiles;
+        if (tile_end > num_tiles) tile_end = num_tiles;
+        if (tile_begin > tile_end || build_failed) tile_begin = tile_end;
+    }
 
     unsigned long long acc = 0;
     // Batches (graph_counts != nullptr): the tiles of graph g are row blocks
@@ -749,8 +764,13 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
         if (threadIdx.x == 0) {
             unsigned long long total = 0;
             for (int w = 0; w < kWarps; ++w) total += s_red[w];
+            if (build_failed) total = ~0ull;
             *scr.result = total;
             if (scr.result2) *scr.result2 = total;
+            if (scr.result_host) {
+                *reinterpret_cast<volatile unsigned long long*>(scr.result_host) = total;
+                __threadfence_system();
+            }
             *scr.done = 0u;
             *scr.work = 0ull;
         }
@@ -759,8 +779,19 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
 
 }  // namespace
 
+// Persistent grid of the count kernel: resident CTAs per SM (the same for every variant:
+// 256 threads at 64 registers and the same shared memory) times the SMs; cached per
+// device and tile width.
 int count_grid_size(int tile_cols)
 {
+    static std::atomic<int> cache[64][2];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) dev = -1;
+    const int w = tile_cols == 128 ? 0 : 1;
+    if (dev >= 0 && dev < 64) {
+        const int v = cache[dev][w].load(std::memory_order_relaxed);
+        if (v > 0) return v;
+    }
     int per_sm = 0;
     cudaError_t e;
     if (tile_cols == 128)
@@ -768,7 +799,9 @@ int count_grid_size(int tile_cols)
     else
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_count<32, false>, kThreads, 0);
     if (e != cudaSuccess || per_sm < 1) per_sm = 1;
-    return per_sm * device_sm_count();
+    const int grid = per_sm * device_sm_count();
+    if (dev >= 0 && dev < 64) cache[dev][w].store(grid, std::memory_order_relaxed);
+    return grid;
 }
 
 int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
@@ -776,12 +809,14 @@ int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
                  int32_t n_row_blocks, int tau, CountScratch scr, cudaStream_t s,
                  const uint32_t* graph_rows, uint32_t num_graphs, unsigned long long* graph_counts,
                  const uint32_t* rowmask, const uint32_t* cellbm, const uint32_t* cellpre,
-                 uint64_t cell_wpr, const uint32_t* row_max, uint32_t tile_begin,
-                 uint32_t tile_end)
+                 uint64_t cell_wpr, const unsigned long long* row_max, uint32_t tile_begin,
+                 uint32_t tile_end, const unsigned long long* build_meta, uint32_t tiles_hint)
 {
+    // build_meta: num_tiles is a capacity bound and the kernel reads the device tile
+    // count; the schedule and the variant follow tiles_hint (the previous build's count)
     if (tile_end > num_tiles) tile_end = num_tiles;
     if (tile_begin > tile_end) tile_begin = tile_end;
-    const uint32_t span = tile_end - tile_begin;
+    const uint32_t span = build_meta ? min(tiles_hint, tile_end - tile_begin) : tile_end - tile_begin;
     const int grid = count_grid_size(tile_cols);
     // Guided schedule: the first round of grabs is about half of an even share per warp
     // (1 to 64 tiles).  Fixed schedule: about an eighth of an even share (8 to 64 tiles);
@@ -795,7 +830,7 @@ int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
     // hold many tiles (long lists to search); meshes and stencils (a few tiles per row
     // block) take the light kernel.
     const bool heavy = rowmask != nullptr && n_row_blocks > 0 &&
-                       (uint64_t)num_tiles >= 8ull * (uint64_t)n_row_blocks;
+                       (uint64_t)(build_meta ? tiles_hint : num_tiles) >= 8ull * (uint64_t)n_row_blocks;
     if (!heavy) {
         rowmask = nullptr;
         cellbm = cellpre = nullptr;
@@ -806,7 +841,7 @@ int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
                                               (uint32_t)chunk, scr,                            \
                                               graph_rows, num_graphs, graph_counts, rowmask,   \
                                               cellbm, cellpre, cell_wpr, (uint32_t)chunk_s, \
-                                              row_max)
+                                              row_max, build_meta)
     if (tile_cols == 128) {
         if (heavy) BTC_LAUNCH_COUNT(128, true);
         else BTC_LAUNCH_COUNT(128, false);

@@ -3,6 +3,18 @@
 
 #include "common.cuh"
 
+// Arguments and buffers of an enqueued build (a cached build graph replays only when
+// they are unchanged).
+constexpr int kBuildKeyPtrs = 19;
+struct BuildGraphKey {
+    const void* ptr[kBuildKeyPtrs];
+    int64_t m;
+    int32_t n;
+    int32_t tile_cols;
+    uint32_t flags;
+    uint32_t cap;
+};
+
 struct btc_bitbsr {
     int device = 0;
     int tile_cols = 0;
@@ -17,9 +29,21 @@ struct btc_bitbsr {
     bool used_bitmap = false;
     // count scratch
     btc200::DevBuf partials, done;
-    unsigned long long* h_meta = nullptr;  // pinned, 8 slots
+    unsigned long long* h_meta = nullptr;  // pinned and mapped, 8 slots
+    unsigned long long* d_hmeta = nullptr; // the device's address of h_meta
     bool edges_known = false;
     int64_t num_edges = 0;
+    // BTC_BUILD_ASYNC: the build is enqueued and its metadata copy to h_meta is marked
+    // by meta_event; num_tiles is the previous build's until resolve_build() has waited.
+    bool pending = false;
+    uint32_t pending_cap = 0;  // tile capacity the enqueued build ran against
+    int failed = 0;  // status of the last build (BTC_OK once resolved without error)
+    cudaEvent_t meta_event = nullptr;
+    // CUDA graph of a repeated asynchronous rebuild (captured on the second identical call)
+    cudaGraphExec_t graph_exec = nullptr;
+    BuildGraphKey graph_key{};
+    BuildGraphKey last_key{};
+    cudaStream_t capture_stream = nullptr;
 
     size_t device_bytes() const
     {
@@ -38,17 +62,29 @@ struct btc_bitbsr {
         for (btc200::DevBuf* b : all) b->release();
         if (h_meta) cudaFreeHost(h_meta);
         h_meta = nullptr;
+        d_hmeta = nullptr;
+        if (meta_event) cudaEventDestroy(meta_event);
+        meta_event = nullptr;
+        pending = false;
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        graph_exec = nullptr;
+        if (capture_stream) cudaStreamDestroy(capture_stream);
+        capture_stream = nullptr;
+        graph_key = BuildGraphKey{};
+        last_key = BuildGraphKey{};
     }
 };
 
+// Waits for an enqueued (BTC_BUILD_ASYNC) build's metadata if one is pending, sets
+// num_tiles and returns the build's status (BTC_E_RANGE, BTC_E_CAPACITY or BTC_OK).
+int resolve_build(btc_bitbsr* g);
 
-// meta slots (device uint64): 0 valid edges, 1 out-of-range ids, 2 tiles, 3 unique
-// edges, 4 vertex count for the degree sort
-enum { kMetaValid = 0, kMetaBad = 1, kMetaTiles = 2, kMetaUniq = 3, kMetaN = 4, kMetaSlots = 8 };
 
 int default_tau(int tile_cols);
 int ensure_count_scratch(btc_bitbsr* g);
 // Counts tiles [tile_begin, tile_end) (clamped to the tile count) into g->result and,
 // when d_out2 is given, *d_out2.
 int count_handle(btc_bitbsr* g, int tau, cudaStream_t s, unsigned long long* d_out2,
-                 uint32_t tile_begin = 0, uint32_t tile_end = 0xffffffffu);
+                 uint32_t tile_begin = 0, uint32_t tile_end = 0xffffffffu, bool to_host = false);
+// Allocates the handle's mapped pinned metadata slots (h_meta, d_hmeta) once.
+int ensure_host_meta(btc_bitbsr* g);

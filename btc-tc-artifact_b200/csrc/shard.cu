@@ -113,6 +113,7 @@ int btc_partition_from_costs(const unsigned long long* bucket_cost, uint64_t n_b
 int btc_partition_tiles(const btc_bitbsr* g, int parts, btc_stream_t stream, uint32_t* bounds)
 {
     if (!g || parts < 1 || !bounds) return BTC_E_INVAL;
+    BTC_TRY(resolve_build(const_cast<btc_bitbsr*>(g)));
     const uint32_t T = g->num_tiles;
     const uint64_t nb = ((uint64_t)T + kCostBucket - 1) / kCostBucket;
     if (nb == 0) return btc_partition_from_costs(nullptr, 0, kCostBucket, 0, parts, bounds);
@@ -141,7 +142,9 @@ int btc_partition_tiles(const btc_bitbsr* g, int parts, btc_stream_t stream, uin
 int btc_count_tiles_async(btc_bitbsr* g, uint32_t tile_begin, uint32_t tile_end, int tau,
                           btc_stream_t stream, unsigned long long* d_out)
 {
-    if (!g || !d_out || tile_begin > tile_end || tile_end > g->num_tiles) return BTC_E_INVAL;
+    if (!g || !d_out) return BTC_E_INVAL;
+    BTC_TRY(resolve_build(g));
+    if (tile_begin > tile_end || tile_end > g->num_tiles) return BTC_E_INVAL;
     return count_handle(g, tau, stream, d_out, tile_begin, tile_end);
 }
 

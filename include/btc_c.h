@@ -37,6 +37,8 @@ typedef struct CUstream_st* btc_stream_t;
 #define BTC_E_CUDA (-3)    /* CUDA runtime error (launch, copy, sync) */
 #define BTC_E_TIMEOUT (-4) /* reserved: a bounded device wait gave up */
 #define BTC_E_RANGE (-5)   /* an input vertex id lies outside [0, n) */
+#define BTC_E_CAPACITY (-6) /* a rebuild enqueued with BTC_BUILD_ASYNC found more tiles
+                               than the handle's arrays hold; nothing was built */
 
 /* Build flags (btc_build_bitbsr, btc_rebuild_bitbsr, btc_convert_*). */
 #define BTC_INPUT_ON_HOST 0x1u /* src/dst are host pointers (pinned or pageable) */
@@ -44,6 +46,7 @@ typedef struct CUstream_st* btc_stream_t;
                                   before orienting each edge to (max, min) */
 #define BTC_BUILD_RADIX 0x4u   /* number tiles with the radix-sort builder even when the
                                   (row block, column block) cell bitmap would fit */
+#define BTC_BUILD_ASYNC 0x8u   /* rebuild without waiting (see btc_rebuild_bitbsr) */
 
 /* Default dense/sparse switch: a tile takes the binary tensor-core path when its
  * popcount exceeds tau.  Pass BTC_TAU_DEFAULT to use the engine's value. */
@@ -139,14 +142,26 @@ typedef struct btc_bitbsr_view {
  * 16 x tile_cols tiles (tile_cols 32 or 128; 0 applies btc_lite_select_tile_cols).
  * Orientation to (max, min), self-loop removal and deduplication happen on the GPU.
  * With BTC_INPUT_ON_HOST the arrays are host memory and are copied on `stream`.
- * Synchronises `stream` once (to size the tile arrays).  *out receives a new handle.
+ * Synchronises `stream` once (to size the tile arrays, or at the end of a rebuild that
+ * fits the handle's arrays).  *out receives a new handle.
  * Limits: n < 2^31, m <= 2^32 - 4096, tiles < 2^32.  Replaces the preprocess + convert pair
  * (convert.h:600, bcsr_16x128.h:136 / bcsr_16x32.h:144). */
 BTC_API int btc_build_bitbsr(const int32_t* src, const int32_t* dst, int64_t m, int32_t n, int tile_cols,
                      uint32_t flags, btc_stream_t stream, btc_bitbsr** out);
 
 /* Same as btc_build_bitbsr into an existing handle, reusing its device buffers
- * when they are large enough (no allocation in steady state). */
+ * when they are large enough (no allocation in steady state).
+ *
+ * BTC_BUILD_ASYNC (no counterpart in the reference): when the handle already holds tile
+ * arrays from an earlier build and the cell-bitmap builder applies, the whole build is
+ * enqueued on `stream` against the arrays' capacity and the call returns without
+ * waiting (otherwise the flag is ignored and the call waits as usual).  The inputs must
+ * stay valid until `stream` has run the build.  A count enqueued after it reads the
+ * tile count on the device.  The build's status arrives with the next call that waits
+ * on the handle (btc_count, btc_bitbsr_info, btc_density_hist, btc_partition_tiles,
+ * btc_count_tiles_async, a rebuild): BTC_E_RANGE for an out-of-range id, BTC_E_CAPACITY
+ * for more tiles than the arrays hold (nothing built; rebuild without the flag).  Until
+ * then a failed build makes btc_count_async write 0xFFFFFFFFFFFFFFFF. */
 BTC_API int btc_rebuild_bitbsr(btc_bitbsr* g, const int32_t* src, const int32_t* dst, int64_t m,
                        int32_t n, int tile_cols, uint32_t flags, btc_stream_t stream);
 

@@ -168,6 +168,138 @@ def test_rebuild_reuses_handle():
     assert g.count() == a["count"]
 
 
+def _arrays_match_oracle(g, name, C_):
+    src, dst, n = golden_graph(name)
+    rp, col, _ = O.lower_csr(src, dst, n)
+    ref = O.bitbsr_build(rp, col, n, C_)
+    h = g.to_host()
+    for k in ("indptr", "indices", "row_indices", "blocks"):
+        assert np.array_equal(np.asarray(h[k]), ref[k]), (name, C_, k)
+
+
+def test_rebuild_sequences_enqueued_against_capacity():
+    """Rebuilds run the whole build against the tile capacity of the previous build and
+    wait once; a graph with more tiles than that capacity redoes the post-count steps.
+    Every step of a sequence that grows, shrinks, switches tile width and hits a bad id
+    must give the oracle's arrays and the golden count."""
+    gold = load_golden()
+    seq = [("stencil27_16", 128), ("stencil27_16", 128), ("K33", 128), ("rmat_12_16_s7", 128),
+           ("rmat_15_16_s7_deg", 128), ("stencil27_4", 32), ("rmat_15_16_s7_deg", 32),
+           ("sbm_600_8_dense", 128), ("rmat_15_16_s7_deg", 128), ("stencil7_16", 32),
+           ("er_5000_32_s5", 128), ("K130", 32)]
+    s0, d0, n0 = golden_graph(seq[0][0])
+    g = BitBSR(_dev(s0), _dev(d0), n0, seq[0][1])
+    for i, (name, C_) in enumerate(seq):
+        s, d, n = golden_graph(name)
+        if i:
+            g.rebuild(_dev(s), _dev(d), n, C_)
+        assert g.num_tiles == gold[name][f"tiles_{C_}"], (i, name, C_)
+        _arrays_match_oracle(g, name, C_)
+        assert g.count() == gold[name]["count"], (i, name, C_)
+        if i == 4:  # a bad id after a good build, then the same graph again
+            bad = np.asarray(s, np.int32).copy()
+            bad[len(bad) // 2] = n + 3
+            with pytest.raises(BtcError) as e:
+                g.rebuild(_dev(bad), _dev(d), n, C_)
+            assert e.value.status == _lib.BTC_E_RANGE
+            g.rebuild(_dev(s), _dev(d), n, C_)
+            assert g.count() == gold[name]["count"]
+    g.free()
+
+
+def test_async_rebuild_pipeline():
+    """BTC_BUILD_ASYNC: rebuilds enqueued without a wait, counted on the device, give the
+    golden counts; the tile count is right once a waiting call resolves the build."""
+    gold = load_golden()
+    s0, d0, n0 = golden_graph("rmat_15_16_s7_deg")  # large first build: room for the rest
+    g = BitBSR(_dev(s0), _dev(d0), n0, 128)
+    out = torch.zeros(1, dtype=torch.int64, device="cuda")
+    for name in ["stencil27_16", "rmat_12_16_s7", "K130", "stencil7_16", "sbm_600_8_dense",
+                 "er_5000_32_s5", "rmat_15_16_s7_deg"]:
+        s, d, n = golden_graph(name)
+        for deg, on_host in ((False, False), (True, True)):
+            src = np.ascontiguousarray(s, np.int32) if on_host else _dev(s)
+            dst = np.ascontiguousarray(d, np.int32) if on_host else _dev(d)
+            g.rebuild(src, dst, n, 128, orient_degree=deg, asynchronous=True)
+            g.count_async(d_out=out.data_ptr())
+            assert int(out.item()) == gold[name]["count"], (name, deg)
+            assert g.count() == gold[name]["count"], (name, deg)
+            if not deg:
+                assert g.num_tiles == gold[name]["tiles_128"]
+                _arrays_match_oracle(g, name, 128)
+    g.free()
+
+
+def test_async_rebuild_graph_replay_follows_buffer_contents():
+    """Identical asynchronous rebuilds (same buffers, sizes, flags) replay a captured
+    CUDA graph from the second repeat on; the graph reads the buffers when it runs, so
+    new contents in the same buffers give their own count."""
+    gold = load_golden()
+    s, d, n = golden_graph("rmat_12_16_s7")
+    want = gold["rmat_12_16_s7"]["count"]
+    ds, dd = _dev(s), _dev(d)
+    g = BitBSR(ds, dd, n, 128)
+    out = torch.zeros(1, dtype=torch.int64, device="cuda")
+    rng = np.random.default_rng(11)
+    for i in range(6):
+        if i >= 3:  # same edges, new order and orientation, written into the same buffers
+            perm = rng.permutation(len(s))
+            flip = rng.random(len(s)) < 0.5
+            ss, dd_ = np.asarray(s)[perm], np.asarray(d)[perm]
+            ds.copy_(torch.from_numpy(np.where(flip, dd_, ss).astype(np.int32)))
+            dd.copy_(torch.from_numpy(np.where(flip, ss, dd_).astype(np.int32)))
+        g.rebuild(ds, dd, n, 128, asynchronous=True)
+        g.count_async(d_out=out.data_ptr())
+        assert int(out.item()) == want, i
+    # a bad id in the replayed buffers surfaces at the next wait, then a fix replays again
+    keep = int(ds[5].item())
+    ds[5] = n + 1
+    g.rebuild(ds, dd, n, 128, asynchronous=True)
+    g.count_async(d_out=out.data_ptr())
+    assert int(out.item()) == -1
+    with pytest.raises(BtcError) as e:
+        g.count()
+    assert e.value.status == _lib.BTC_E_RANGE
+    ds[5] = keep
+    for _ in range(2):
+        g.rebuild(ds, dd, n, 128, asynchronous=True)
+        assert g.count() == want
+    _arrays_match_oracle(g, "rmat_12_16_s7", 128)
+    g.free()
+
+
+def test_async_rebuild_failures_surface_at_next_wait():
+    gold = load_golden()
+    s, d, n = golden_graph("stencil27_16")
+    g = BitBSR(_dev(s), _dev(d), n, 128)
+    out = torch.zeros(1, dtype=torch.int64, device="cuda")
+    # an out-of-range id: the enqueued count writes all ones, the next wait reports it
+    bad = np.asarray(s, np.int32).copy()
+    bad[7] = n
+    g.rebuild(_dev(bad), _dev(d), n, 128, asynchronous=True)
+    g.count_async(d_out=out.data_ptr())
+    assert int(out.item()) == -1
+    with pytest.raises(BtcError) as e:
+        g.count()
+    assert e.value.status == _lib.BTC_E_RANGE
+    with pytest.raises(BtcError):
+        g.count()  # the handle stays failed until a good rebuild
+    g.rebuild(_dev(s), _dev(d), n, 128, asynchronous=True)
+    assert g.count() == gold["stencil27_16"]["count"]
+    # more tiles than the arrays hold: nothing built, BTC_E_CAPACITY, then a waiting
+    # rebuild of the same graph succeeds
+    s2, d2, n2 = golden_graph("rmat_15_16_s7_deg")
+    g.rebuild(_dev(s2), _dev(d2), n2, 128, asynchronous=True)
+    g.count_async(d_out=out.data_ptr())
+    assert int(out.item()) == -1
+    with pytest.raises(BtcError) as e:
+        g.info()
+    assert e.value.status == _lib.BTC_E_CAPACITY
+    g.rebuild(_dev(s2), _dev(d2), n2, 128)
+    assert g.count() == gold["rmat_15_16_s7_deg"]["count"]
+    g.free()
+
+
 def test_count_async_device_output():
     s, d, n = golden_graph("rmat_10_8_s11")
     fx = load_golden()["rmat_10_8_s11"]
