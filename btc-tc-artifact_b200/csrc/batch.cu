@@ -429,7 +429,7 @@ int btc_batch_count(btc_batch* b, int tau, btc_stream_t stream, unsigned long lo
                          g->row_indices.as<uint32_t>(), g->blocks.as<uint32_t>(), g->num_tiles,
                          g->n_row_blocks, tau, scr, stream, b->row_off.as<uint32_t>(),
                          (uint32_t)b->num_graphs, counts, g->rowmask.as<uint32_t>(), nullptr,
-                         nullptr, 0, g->meta.as<unsigned long long>() + kMetaRowMax));
+                         0, g->meta.as<unsigned long long>() + kMetaRowMax));
     if (h_counts) {
         BTC_CUDA_TRY(cudaMemcpyAsync(h_counts, counts, bytes, cudaMemcpyDeviceToHost, stream));
         BTC_CUDA_TRY(cudaStreamSynchronize(stream));

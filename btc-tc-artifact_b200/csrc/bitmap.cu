@@ -199,7 +199,7 @@ __device__ __forceinline__ void finish_tiles(uint32_t* indptr, int32_t R, unsign
 
 __global__ void __launch_bounds__(kThreads)
 k_bm_emit(const uint32_t* __restrict__ bitmap, uint64_t W, uint64_t wpr,
-          const uint32_t* __restrict__ chunk_base, uint32_t* __restrict__ prefix,
+          const uint32_t* __restrict__ chunk_base, uint2* __restrict__ cellpp,
           uint32_t* __restrict__ indices, uint32_t* __restrict__ row_indices,
           uint32_t* __restrict__ indptr, unsigned long long* meta, uint32_t cap,
           unsigned long long* host_meta, int32_t R, uint4* __restrict__ blocks, uint32_t tile_vec4)
@@ -261,14 +261,14 @@ k_bm_emit(const uint32_t* __restrict__ bitmap, uint64_t W, uint64_t wpr,
         }
     }
     if (w0 + kWordsPerThread <= W) {
-        uint4* p = reinterpret_cast<uint4*>(prefix + w0);
+        uint4* p = reinterpret_cast<uint4*>(cellpp + w0);
 #pragma unroll
-        for (int q = 0; q < kWordsPerThread / 4; ++q)
-            p[q] = make_uint4(pre[4 * q], pre[4 * q + 1], pre[4 * q + 2], pre[4 * q + 3]);
+        for (int q = 0; q < kWordsPerThread / 2; ++q)
+            p[q] = make_uint4(x[2 * q], pre[2 * q], x[2 * q + 1], pre[2 * q + 1]);
     } else {
 #pragma unroll
         for (int k = 0; k < kWordsPerThread; ++k)
-            if (w0 + k < W) prefix[w0 + k] = pre[k];
+            if (w0 + k < W) cellpp[w0 + k] = make_uint2(x[k], pre[k]);
     }
 }
 
@@ -276,7 +276,7 @@ template <int LOG2C>
 __global__ void __launch_bounds__(kThreads)
 k_fill_bm(const int32_t* __restrict__ src, const int32_t* __restrict__ dst, int64_t m, int32_t n,
           const int32_t* __restrict__ rank, uint64_t wpr, const uint32_t* __restrict__ bitmap,
-          const uint32_t* __restrict__ prefix, uint32_t* __restrict__ blocks,
+          const uint2* __restrict__ cellpp, uint32_t* __restrict__ blocks,
           const unsigned long long* __restrict__ d_tiles, uint32_t cap)
 {
     if (*d_tiles > cap) return;  // overflowed tile arrays: the builder redoes this step
@@ -305,8 +305,9 @@ k_fill_bm(const int32_t* __restrict__ src, const int32_t* __restrict__ dst, int6
 #pragma unroll
         for (int k = 0; k < U; ++k) {
             const uint64_t w = (uint64_t)(r[k] >> 4) * wpr + ((c[k] >> LOG2C) >> 5);
-            pre[k] = ok[k] ? prefix[w] : 0u;
-            word[k] = ok[k] ? bitmap[w] : 0u;
+            const uint2 cp = ok[k] ? cellpp[w] : make_uint2(0u, 0u);
+            word[k] = cp.x;
+            pre[k] = cp.y;
         }
 #pragma unroll
         for (int k = 0; k < U; ++k) {
@@ -388,7 +389,7 @@ int bitmap_mark_and_count(const BuildGeom& g, const int32_t* src, const int32_t*
 
 int bitmap_emit_and_fill(const BuildGeom& g, const int32_t* src, const int32_t* dst, int64_t m,
                          const int32_t* rank, const uint32_t* bitmap, const uint32_t* chunk_base,
-                         uint32_t* prefix, uint32_t* indices, uint32_t* row_indices,
+                         uint2* cellpp, uint32_t* indices, uint32_t* row_indices,
                          uint32_t* indptr, uint32_t* blocks, unsigned long long* meta,
                          uint32_t cap, unsigned long long* host_meta, cudaStream_t s)
 {
@@ -398,17 +399,17 @@ int bitmap_emit_and_fill(const BuildGeom& g, const int32_t* src, const int32_t* 
     const uint32_t vec4 = 4u * (uint32_t)(g.tile_cols / 32);  // 16-byte words per tile
     if (W > 0)
         bm::k_bm_emit<<<(unsigned)bitmap_chunks(W), bm::kThreads, 0, s>>>(
-            bitmap, W, wpr, chunk_base, prefix, indices, row_indices, indptr, meta, cap,
+            bitmap, W, wpr, chunk_base, cellpp, indices, row_indices, indptr, meta, cap,
             host_meta, g.n_row_blocks, reinterpret_cast<uint4*>(blocks), vec4);
     else
         bm::k_set_last<<<1, 1, 0, s>>>(indptr, g.n_row_blocks, meta, cap, host_meta);
     if (m > 0 && W > 0) {
         if (g.tile_cols == 128)
             bm::k_fill_bm<7><<<edge_grid(m), bm::kThreads, 0, s>>>(
-                src, dst, m, g.n, rank, wpr, bitmap, prefix, blocks, meta_tiles, cap);
+                src, dst, m, g.n, rank, wpr, bitmap, cellpp, blocks, meta_tiles, cap);
         else
             bm::k_fill_bm<5><<<edge_grid(m), bm::kThreads, 0, s>>>(
-                src, dst, m, g.n, rank, wpr, bitmap, prefix, blocks, meta_tiles, cap);
+                src, dst, m, g.n, rank, wpr, bitmap, cellpp, blocks, meta_tiles, cap);
     }
     return cudaGetLastError() == cudaSuccess ? BTC_OK : BTC_E_CUDA;
 }
@@ -456,6 +457,9 @@ __global__ void k_rowmask(const uint32_t* __restrict__ blocks, uint32_t cap,
         mx = max(mx, indptr[i + 1] - indptr[i]);
     mx = __reduce_max_sync(kFull, mx);
     if ((threadIdx.x & 31) == 0 && mx) atomicMax(row_max, (unsigned long long)mx);
+    // the masks serve only the heavy count variant, which reads them only when row
+    // blocks average 8 or more tiles (the same test on the same count)
+    if ((uint64_t)num_tiles < 8ull * (uint64_t)R) return;
 
     for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < num_tiles;
          t += (uint64_t)gridDim.x * blockDim.x) {

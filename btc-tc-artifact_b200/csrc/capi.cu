@@ -28,7 +28,7 @@ size_t bitmap_chunks(uint64_t W);
 int bitmap_mark_and_count(const BuildGeom&, const int32_t*, const int32_t*, int64_t, const int32_t*,
                           uint32_t*, uint32_t*, unsigned long long*, unsigned long long*, cudaStream_t);
 int bitmap_emit_and_fill(const BuildGeom&, const int32_t*, const int32_t*, int64_t, const int32_t*,
-                         const uint32_t*, const uint32_t*, uint32_t*, uint32_t*, uint32_t*, uint32_t*,
+                         const uint32_t*, const uint32_t*, uint2*, uint32_t*, uint32_t*, uint32_t*,
                          uint32_t*, unsigned long long*, uint32_t, unsigned long long*,
                          cudaStream_t);
 int launch_popcount_sum(int, const uint32_t*, uint64_t, unsigned long long*, cudaStream_t);
@@ -167,7 +167,7 @@ static int enqueue_build(btc_bitbsr* g, const BuildPlan& P, uint64_t** sorted_ou
         if (P.cap) {
             BTC_TRY(bitmap_emit_and_fill(geom, P.d_src, P.d_dst, P.m, rank,
                                          g->bitmap.as<uint32_t>(), g->tile_base.as<uint32_t>(),
-                                         g->prefix.as<uint32_t>(), g->indices.as<uint32_t>(),
+                                         g->prefix.as<uint2>(), g->indices.as<uint32_t>(),
                                          g->row_indices.as<uint32_t>(), g->indptr.as<uint32_t>(),
                                          g->blocks.as<uint32_t>(), meta, P.cap, g->d_hmeta, s));
             BTC_TRY(launch_rowmask(geom.tile_cols, g->blocks.as<uint32_t>(), P.cap,
@@ -308,7 +308,7 @@ static int build_into(btc_bitbsr* g, const int32_t* src, const int32_t* dst, int
     }
     if (P.use_bitmap) {
         BTC_TRY(g->bitmap.reserve(sizeof(uint32_t) * (P.bm_words ? P.bm_words : 1)));
-        BTC_TRY(g->prefix.reserve(sizeof(uint32_t) * (P.bm_words ? P.bm_words : 1)));
+        BTC_TRY(g->prefix.reserve(sizeof(uint2) * (P.bm_words ? P.bm_words : 1)));
     }
     BTC_TRY(g->indptr.reserve(sizeof(uint32_t) * ((size_t)geom.n_row_blocks + 1)));
     BTC_TRY(ensure_count_scratch(g));
@@ -363,7 +363,7 @@ static int build_into(btc_bitbsr* g, const int32_t* src, const int32_t* dst, int
     if (P.use_bitmap) {
         BTC_TRY(bitmap_emit_and_fill(geom, P.d_src, P.d_dst, m, P.degree ? g->rank.as<int32_t>() : nullptr,
                                      g->bitmap.as<uint32_t>(), g->tile_base.as<uint32_t>(),
-                                     g->prefix.as<uint32_t>(), g->indices.as<uint32_t>(),
+                                     g->prefix.as<uint2>(), g->indices.as<uint32_t>(),
                                      g->row_indices.as<uint32_t>(), g->indptr.as<uint32_t>(),
                                      g->blocks.as<uint32_t>(), meta, (uint32_t)tiles, nullptr, s));
     } else {
@@ -404,8 +404,7 @@ int count_handle(btc_bitbsr* g, int tau, cudaStream_t s, unsigned long long* d_o
                         g->row_indices.as<uint32_t>(), g->blocks.as<uint32_t>(),
                         g->pending ? g->pending_cap : g->num_tiles, g->n_row_blocks, tau, scr, s,
                         nullptr, 0, nullptr, g->rowmask.as<uint32_t>(),
-                        g->used_bitmap ? g->bitmap.as<uint32_t>() : nullptr,
-                        g->used_bitmap ? g->prefix.as<uint32_t>() : nullptr,
+                        g->used_bitmap ? g->prefix.as<uint2>() : nullptr,
                         bitmap_words_per_row(make_geom(g->n, g->tile_cols)),
                         g->meta.as<unsigned long long>() + kMetaRowMax, tile_begin, tile_end,
                         build_meta, g->num_tiles);

@@ -154,15 +154,16 @@ int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
                  int32_t n_row_blocks, int tau, CountScratch scr, cudaStream_t s,
                  const uint32_t* graph_rows = nullptr, uint32_t num_graphs = 0,
                  unsigned long long* graph_counts = nullptr, const uint32_t* rowmask = nullptr,
-                 const uint32_t* cellbm = nullptr, const uint32_t* cellpre = nullptr,
+                 const uint2* cellpp = nullptr,
                  uint64_t cell_wpr = 0, const unsigned long long* row_max = nullptr,
                  uint32_t tile_begin = 0, uint32_t tile_end = 0xffffffffu,
                  const unsigned long long* build_meta = nullptr, uint32_t tiles_hint = 0);
 
 // rowmask[t] bit r = tile t's row r has a bit, for t < T = *d_tiles (T = cap when d_tiles
-// is null), and *row_max = max(*row_max, the most tiles in one row block), which picks
-// the count kernel's schedule (the caller zeroes it).  Runs after the tiles are filled.
-// Writes nothing when T > cap (the tile arrays overflowed).
+// is null) when T >= 8 * n_row_blocks (the heavy count variant's condition), and
+// *row_max = max(*row_max, the most tiles in one row block), which picks the count
+// kernel's schedule (the caller zeroes it).  Runs after the tiles are filled.  Writes
+// nothing when T > cap (the tile arrays overflowed).
 int launch_rowmask(int tile_cols, const uint32_t* blocks, uint32_t cap,
                    const unsigned long long* d_tiles, const uint32_t* indptr, int32_t n_row_blocks,
                    uint32_t* rowmask, unsigned long long* row_max, cudaStream_t s);

@@ -58,7 +58,6 @@ struct Cfg {
     static constexpr int WPR = C / 32;       // words per tile row
     static constexpr int TW = 16 * WPR;      // words per tile
     static constexpr int JPT = C / 16;       // 16-row blocks covered by a tile's columns
-    static constexpr int MAXBITS = 16 * C;   // bits per tile
 };
 
 template <int C>
@@ -338,7 +337,7 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
         uint32_t chunk, CountScratch scr,
         const uint32_t* __restrict__ graph_rows, uint32_t num_graphs,
         unsigned long long* __restrict__ graph_counts, const uint32_t* __restrict__ rowmask,
-        const uint32_t* __restrict__ cellbm, const uint32_t* __restrict__ cellpre, uint64_t cell_wpr,
+        const uint2* __restrict__ cellpp, uint64_t cell_wpr,
         uint32_t chunk_skewed, const unsigned long long* __restrict__ row_max,
         const unsigned long long* __restrict__ build_meta)
 {
@@ -364,6 +363,9 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
         if (tile_end > num_tiles) tile_end = num_tiles;
         if (tile_begin > tile_end || build_failed) tile_begin = tile_end;
     }
+
+    // row-occupancy masks exist only when row blocks average 8 or more tiles
+    if ((uint64_t)num_tiles < 8ull * (uint64_t)(R > 0 ? R : 0)) rowmask = nullptr;
 
     unsigned long long acc = 0;
     // Batches (graph_counts != nullptr): the tiles of graph g are row blocks
@@ -560,7 +562,7 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
                     const uint32_t jb = s.jptr[lane], je = s.jptr[lane + 1];
                     len = je - jb;
                     start = jb;
-                    if (heavy && cellbm && je > jb) {
+                    if (heavy && cellpp && je > jb) {
                         const uint32_t r0 = a_rank<C>(s, A, indices, indices[jb]);
                         const uint32_t r1 = a_rank<C>(s, A, indices, indices[je - 1] + 1);
                         if (r1 - r0 < len) {
@@ -614,9 +616,10 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
                             pa = idx;
                             const uint32_t a = indices[pa];
                             const uint64_t cw = (uint64_t)(JL * JPT + jsel) * cell_wpr + (a >> 5);
-                            const uint32_t x = cellbm[cw], bit = 1u << (a & 31u);
-                            found = (x & bit) != 0u;
-                            if (found) pb = cellpre[cw] + __popc(x & (bit - 1u));
+                            const uint2 cp = cellpp[cw];
+                            const uint32_t bit = 1u << (a & 31u);
+                            found = (cp.x & bit) != 0u;
+                            if (found) pb = cp.y + __popc(cp.x & (bit - 1u));
                         }
                         if (found && rmask_g) {
                             ra = rmask_g[pa];
@@ -808,7 +811,7 @@ int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
                  const uint32_t* row_indices, const uint32_t* blocks, uint32_t num_tiles,
                  int32_t n_row_blocks, int tau, CountScratch scr, cudaStream_t s,
                  const uint32_t* graph_rows, uint32_t num_graphs, unsigned long long* graph_counts,
-                 const uint32_t* rowmask, const uint32_t* cellbm, const uint32_t* cellpre,
+                 const uint32_t* rowmask, const uint2* cellpp,
                  uint64_t cell_wpr, const unsigned long long* row_max, uint32_t tile_begin,
                  uint32_t tile_end, const unsigned long long* build_meta, uint32_t tiles_hint)
 {
@@ -833,14 +836,14 @@ int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
                        (uint64_t)(build_meta ? tiles_hint : num_tiles) >= 8ull * (uint64_t)n_row_blocks;
     if (!heavy) {
         rowmask = nullptr;
-        cellbm = cellpre = nullptr;
+        cellpp = nullptr;
     }
 #define BTC_LAUNCH_COUNT(CC, HH)                                                              \
     k_count<CC, HH><<<grid, kThreads, 0, s>>>(indptr, indices, row_indices, blocks, num_tiles, \
                                               tile_begin, tile_end, n_row_blocks, tau,         \
                                               (uint32_t)chunk, scr,                            \
                                               graph_rows, num_graphs, graph_counts, rowmask,   \
-                                              cellbm, cellpre, cell_wpr, (uint32_t)chunk_s, \
+                                              cellpp, cell_wpr, (uint32_t)chunk_s,             \
                                               row_max, build_meta)
     if (tile_cols == 128) {
         if (heavy) BTC_LAUNCH_COUNT(128, true);
