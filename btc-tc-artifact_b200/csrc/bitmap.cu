@@ -87,23 +87,26 @@ k_mark(const int32_t* __restrict__ src, const int32_t* __restrict__ dst, int64_t
 }
 
 // Per-thread view of 16 consecutive bitmap words.
-__device__ __forceinline__ void load16(const uint32_t* __restrict__ bitmap, uint64_t w0, uint64_t W,
-                                       uint32_t (&x)[kWordsPerThread])
+template <int WPT>
+__device__ __forceinline__ void load_words(const uint32_t* __restrict__ bitmap, uint64_t w0,
+                                           uint64_t W, uint32_t (&x)[WPT])
 {
-    if (w0 + kWordsPerThread <= W) {
-        const uint4* p = reinterpret_cast<const uint4*>(bitmap + w0);
+    if constexpr (WPT % 4 == 0) {
+        if (w0 + WPT <= W) {
+            const uint4* p = reinterpret_cast<const uint4*>(bitmap + w0);
 #pragma unroll
-        for (int q = 0; q < kWordsPerThread / 4; ++q) {
-            const uint4 v = p[q];
-            x[4 * q] = v.x;
-            x[4 * q + 1] = v.y;
-            x[4 * q + 2] = v.z;
-            x[4 * q + 3] = v.w;
+            for (int q = 0; q < WPT / 4; ++q) {
+                const uint4 v = p[q];
+                x[4 * q] = v.x;
+                x[4 * q + 1] = v.y;
+                x[4 * q + 2] = v.z;
+                x[4 * q + 3] = v.w;
+            }
+            return;
         }
-    } else {
-#pragma unroll
-        for (int k = 0; k < kWordsPerThread; ++k) x[k] = (w0 + k < W) ? bitmap[w0 + k] : 0u;
     }
+#pragma unroll
+    for (int k = 0; k < WPT; ++k) x[k] = (w0 + k < W) ? bitmap[w0 + k] : 0u;
 }
 
 __global__ void __launch_bounds__(kThreads)
@@ -112,7 +115,7 @@ k_bm_count(const uint32_t* __restrict__ bitmap, uint64_t W, uint32_t* __restrict
     __shared__ uint32_t s_warp[kThreads / kWarp];
     const uint64_t w0 = (uint64_t)blockIdx.x * kChunk + (uint64_t)threadIdx.x * kWordsPerThread;
     uint32_t x[kWordsPerThread];
-    load16(bitmap, w0, W, x);
+    load_words<kWordsPerThread>(bitmap, w0, W, x);
     uint32_t s = 0;
 #pragma unroll
     for (int k = 0; k < kWordsPerThread; ++k) s += __popc(x[k]);
@@ -129,6 +132,7 @@ k_bm_count(const uint32_t* __restrict__ bitmap, uint64_t W, uint32_t* __restrict
 // Chunk popcounts into chunk_base[b]; the last CTA to finish (a ticket in
 // meta[kMetaTicket], zeroed with the metadata) scans them in place into exclusive chunk
 // bases and writes the tile total to meta[kMetaTiles].  No CTA waits for another.
+template <int WPT>
 __global__ void __launch_bounds__(kThreads)
 k_bm_count_scan(const uint32_t* __restrict__ bitmap, uint64_t W, uint32_t* chunk_base,
                 unsigned long long* meta)
@@ -137,12 +141,12 @@ k_bm_count_scan(const uint32_t* __restrict__ bitmap, uint64_t W, uint32_t* chunk
     __shared__ unsigned long long s_tot[kThreads / kWarp];
     __shared__ int s_last;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint64_t w0 = (uint64_t)blockIdx.x * kChunk + (uint64_t)threadIdx.x * kWordsPerThread;
-    uint32_t x[kWordsPerThread];
-    load16(bitmap, w0, W, x);
+    const uint64_t w0 = (uint64_t)blockIdx.x * (kThreads * WPT) + (uint64_t)threadIdx.x * WPT;
+    uint32_t x[WPT];
+    load_words<WPT>(bitmap, w0, W, x);
     uint32_t sum = 0;
 #pragma unroll
-    for (int k = 0; k < kWordsPerThread; ++k) sum += __popc(x[k]);
+    for (int k = 0; k < WPT; ++k) sum += __popc(x[k]);
     sum = __reduce_add_sync(kFull, sum);
     if (lane == 0) s_warp[warp] = sum;
     __syncthreads();
@@ -197,6 +201,7 @@ __device__ __forceinline__ void finish_tiles(uint32_t* indptr, int32_t R, unsign
     }
 }
 
+template <int WPT>
 __global__ void __launch_bounds__(kThreads)
 k_bm_emit(const uint32_t* __restrict__ bitmap, uint64_t W, uint64_t wpr,
           const uint32_t* __restrict__ chunk_base, uint2* __restrict__ cellpp,
@@ -216,12 +221,12 @@ k_bm_emit(const uint32_t* __restrict__ bitmap, uint64_t W, uint64_t wpr,
             blocks[i] = make_uint4(0u, 0u, 0u, 0u);
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint64_t w0 = (uint64_t)blockIdx.x * kChunk + (uint64_t)threadIdx.x * kWordsPerThread;
-    uint32_t x[kWordsPerThread];
-    load16(bitmap, w0, W, x);
+    const uint64_t w0 = (uint64_t)blockIdx.x * (kThreads * WPT) + (uint64_t)threadIdx.x * WPT;
+    uint32_t x[WPT];
+    load_words<WPT>(bitmap, w0, W, x);
     uint32_t mine = 0;
 #pragma unroll
-    for (int k = 0; k < kWordsPerThread; ++k) mine += __popc(x[k]);
+    for (int k = 0; k < WPT; ++k) mine += __popc(x[k]);
     // exclusive prefix of `mine` over the CTA (thread order = word order)
     uint32_t incl = mine;
 #pragma unroll
@@ -238,9 +243,9 @@ k_bm_emit(const uint32_t* __restrict__ bitmap, uint64_t W, uint64_t wpr,
 
     uint64_t rb = w0 / wpr;
     uint64_t col_word = w0 - rb * wpr;
-    uint32_t pre[kWordsPerThread];
+    uint32_t pre[WPT];
 #pragma unroll
-    for (int k = 0; k < kWordsPerThread; ++k) {
+    for (int k = 0; k < WPT; ++k) {
         pre[k] = base;
         if (w0 + k < W) {
             if (col_word == 0) indptr[rb] = base;
@@ -260,14 +265,14 @@ k_bm_emit(const uint32_t* __restrict__ bitmap, uint64_t W, uint64_t wpr,
             ++rb;
         }
     }
-    if (w0 + kWordsPerThread <= W) {
+    if (WPT % 2 == 0 && w0 + WPT <= W) {
         uint4* p = reinterpret_cast<uint4*>(cellpp + w0);
 #pragma unroll
-        for (int q = 0; q < kWordsPerThread / 2; ++q)
+        for (int q = 0; q < WPT / 2; ++q)
             p[q] = make_uint4(x[2 * q], pre[2 * q], x[2 * q + 1], pre[2 * q + 1]);
     } else {
 #pragma unroll
-        for (int k = 0; k < kWordsPerThread; ++k)
+        for (int k = 0; k < WPT; ++k)
             if (w0 + k < W) cellpp[w0 + k] = make_uint2(x[k], pre[k]);
     }
 }
@@ -357,7 +362,22 @@ uint64_t bitmap_words_per_row(const BuildGeom& g)
     return (uint64_t)((g.n_col_blocks + 31) / 32);
 }
 
-size_t bitmap_chunks(uint64_t W) { return (size_t)((W + bm::kChunk - 1) / bm::kChunk); }
+// Words per thread of the chunk popcount/scan and emit: 16 when that still gives two CTAs
+// per SM, else 4, else 1 (small bitmaps with many tiles per word: the per-CTA share of
+// emitted and zeroed tiles stays small).
+static int bitmap_wpt(uint64_t W)
+{
+    const uint64_t ctas = 2ull * (uint64_t)device_sm_count();
+    if (W / (bm::kThreads * 16ull) >= ctas) return 16;
+    if (W / (bm::kThreads * 4ull) >= ctas) return 4;
+    return 1;
+}
+
+size_t bitmap_chunks(uint64_t W)
+{
+    const uint64_t chunk = (uint64_t)bm::kThreads * bitmap_wpt(W);
+    return (size_t)((W + chunk - 1) / chunk);
+}
 
 int bitmap_mark_and_count(const BuildGeom& g, const int32_t* src, const int32_t* dst, int64_t m,
                           const int32_t* rank, uint32_t* bitmap, uint32_t* chunk_count,
@@ -382,8 +402,18 @@ int bitmap_mark_and_count(const BuildGeom& g, const int32_t* src, const int32_t*
     }
     const size_t chunks = bitmap_chunks(W);
     // meta_tiles - kMetaTiles is the metadata base (its ticket slot is zero)
-    bm::k_bm_count_scan<<<(unsigned)chunks, bm::kThreads, 0, s>>>(bitmap, W, chunk_count,
-                                                                   meta_tiles - kMetaTiles);
+    unsigned long long* meta = meta_tiles - kMetaTiles;
+    switch (bitmap_wpt(W)) {
+    case 16:
+        bm::k_bm_count_scan<16><<<(unsigned)chunks, bm::kThreads, 0, s>>>(bitmap, W, chunk_count, meta);
+        break;
+    case 4:
+        bm::k_bm_count_scan<4><<<(unsigned)chunks, bm::kThreads, 0, s>>>(bitmap, W, chunk_count, meta);
+        break;
+    default:
+        bm::k_bm_count_scan<1><<<(unsigned)chunks, bm::kThreads, 0, s>>>(bitmap, W, chunk_count, meta);
+        break;
+    }
     return cudaGetLastError() == cudaSuccess ? BTC_OK : BTC_E_CUDA;
 }
 
@@ -397,10 +427,21 @@ int bitmap_emit_and_fill(const BuildGeom& g, const int32_t* src, const int32_t* 
     const uint64_t wpr = bitmap_words_per_row(g);
     const uint64_t W = wpr * (uint64_t)g.n_row_blocks;
     const uint32_t vec4 = 4u * (uint32_t)(g.tile_cols / 32);  // 16-byte words per tile
-    if (W > 0)
-        bm::k_bm_emit<<<(unsigned)bitmap_chunks(W), bm::kThreads, 0, s>>>(
-            bitmap, W, wpr, chunk_base, cellpp, indices, row_indices, indptr, meta, cap,
-            host_meta, g.n_row_blocks, reinterpret_cast<uint4*>(blocks), vec4);
+    if (W > 0) {
+        const unsigned grid = (unsigned)bitmap_chunks(W);
+        uint4* b4 = reinterpret_cast<uint4*>(blocks);
+        const int R = g.n_row_blocks;
+#define BTC_EMIT(WPT)                                                                         \
+    bm::k_bm_emit<WPT><<<grid, bm::kThreads, 0, s>>>(bitmap, W, wpr, chunk_base, cellpp, indices, \
+                                                    row_indices, indptr, meta, cap, host_meta, R, \
+                                                    b4, vec4)
+        switch (bitmap_wpt(W)) {
+        case 16: BTC_EMIT(16); break;
+        case 4: BTC_EMIT(4); break;
+        default: BTC_EMIT(1); break;
+        }
+#undef BTC_EMIT
+    }
     else
         bm::k_set_last<<<1, 1, 0, s>>>(indptr, g.n_row_blocks, meta, cap, host_meta);
     if (m > 0 && W > 0) {
@@ -432,9 +473,12 @@ int launch_popcount_sum(int tile_cols, const uint32_t* blocks, uint64_t num_tile
 }  // namespace btc200
 
 namespace btc200 {
+// Popcount per fixed 4096-word chunk (bm::kChunk; the batch builder's chunking, which
+// does not follow bitmap_chunks).
 int launch_bitmap_count(const uint32_t* bitmap, uint64_t W, uint32_t* chunk_count, cudaStream_t s)
 {
-    if (W) bm::k_bm_count<<<(unsigned)bitmap_chunks(W), bm::kThreads, 0, s>>>(bitmap, W, chunk_count);
+    const uint64_t chunks = (W + bm::kChunk - 1) / bm::kChunk;
+    if (W) bm::k_bm_count<<<(unsigned)chunks, bm::kThreads, 0, s>>>(bitmap, W, chunk_count);
     return cudaGetLastError() == cudaSuccess ? BTC_OK : BTC_E_CUDA;
 }
 }  // namespace btc200

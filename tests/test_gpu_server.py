@@ -54,19 +54,21 @@ def test_counts_same_alone_and_in_the_mix(slots, max_graphs, borrow):
     rng = np.random.default_rng(slots * 100 + max_graphs)
     order = list(rng.permutation(len(gs))) * 3
     srv = Server(slots=slots, max_batch_graphs=max_graphs)
-    for k, c in _run(srv, gs, order, gap_s=0.0005, borrow=borrow):
-        assert c == want[k]
-    st = srv.stats()
-    assert st["graphs"] == len(order) and st["rejected"] == 0
-    if max_graphs > 1:
-        # a burst of submissions (no gaps) queues behind the running batches, so the
-        # engine must put several requests in one batch
-        for k, c in _run(srv, gs, order, gap_s=0.0, borrow=borrow):
+    try:
+        for k, c in _run(srv, gs, order, gap_s=0.0005, borrow=borrow):
             assert c == want[k]
-        st2 = srv.stats()
-        assert st2["graphs"] == 2 * len(order)
-        assert st2["batches"] - st["batches"] < len(order)
-    srv.close()
+        st = srv.stats()
+        assert st["graphs"] == len(order) and st["rejected"] == 0
+        if max_graphs > 1:
+            # a burst of submissions (no gaps) queues behind the running batches, so the
+            # engine must put several requests in one batch
+            for k, c in _run(srv, gs, order, gap_s=0.0, borrow=borrow):
+                assert c == want[k]
+            st2 = srv.stats()
+            assert st2["graphs"] == 2 * len(order)
+            assert st2["batches"] - st["batches"] < len(order)
+    finally:
+        srv.close()
 
 
 def test_budget_rejects_a_request_too_large_alone():
