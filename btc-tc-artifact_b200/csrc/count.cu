@@ -272,7 +272,7 @@ __device__ __forceinline__ unsigned long long bit_pass(WarpSmem<C>& s, uint32_t 
                 const uint32_t k0 = max(s.mc[j], lo), k1 = min(s.mc[j + 1], hi);
                 const uint32_t* Ar = blocks + r * WPR;
                 const uint32_t* Br = blocks + c * WPR;
-#pragma unroll 2
+#pragma unroll(kHeavy ? 1 : 2)
                 for (uint32_t k = k0 + lane; k < k1; k += kWarp) {
                     if (kHeavy && !((s.mra[k - lo] >> r) & (s.mrb[k - lo] >> c) & 1u)) continue;
                     const size_t pa = s.mpa[k - lo], pb = s.mpb[k - lo];
@@ -295,7 +295,7 @@ __device__ __forceinline__ unsigned long long bit_pass(WarpSmem<C>& s, uint32_t 
                 const uint32_t k0 = max(s.mc[j], lo), k1 = min(s.mc[j + 1], hi);
                 const uint32_t* Ar = blocks + r * WPR;
                 const uint32_t* Br = blocks + c * WPR;
-#pragma unroll 2
+#pragma unroll(kHeavy ? 1 : 2)
                 for (uint32_t k = k0; k < k1; ++k) {
                     if (kHeavy && !((s.mra[k - lo] >> r) & (s.mrb[k - lo] >> c) & 1u)) continue;
                     const size_t pa = s.mpa[k - lo], pb = s.mpb[k - lo];
@@ -460,7 +460,9 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
                 grab_range(__shfl_sync(kFull, kq, 0), tn, cen);
                 if (tn < tile_end) load_ids(tn, nI, nJL, nw0, nw1);
                 nstate = 3;
-            } else if (nstate == 0) {
+            } else if (nstate == 0 && !kHeavy) {
+                // (heavy tiles are long: holding the next tile's words across one costs
+                // more than the load it saves, so the heavy variant loads them at the top)
                 nptrs = load_ptrs(nI, nJL);
                 nstate = 1;
             }
