@@ -209,6 +209,81 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def dense_triples(h, tile_cols: int, tau: int) -> int:
+    """(tile, slice, matched column block) triples of the tiles whose popcount exceeds tau:
+    each is two m16n8k128 binary MMAs (16 x 16 x 128 AND-popcount-accumulates) on the
+    count kernel's dense path."""
+    jpt = tile_cols // 16
+    wpr = tile_cols // 32
+    indptr, indices, rows = h["indptr"], h["indices"], h["row_indices"]
+    blocks = h["blocks"].reshape(-1, 16, wpr)
+    R = len(indptr) - 1
+    total = 0
+    for t in range(len(indices)):
+        tile = blocks[t]
+        if int(np.unpackbits(tile.view(np.uint8)).sum()) <= tau:
+            continue
+        I, JL = int(rows[t]), int(indices[t])
+        la = indices[indptr[I]:indptr[I + 1]]
+        for j in range(jpt):
+            J = JL * jpt + j
+            if J >= R:
+                break
+            sl = (tile[:, (16 * j) // 32] >> np.uint32((16 * j) % 32)) & np.uint32(0xFFFF)
+            if not sl.any():
+                continue
+            total += len(np.intersect1d(la, indices[indptr[J]:indptr[J + 1]],
+                                        assume_unique=True))
+    return total
+
+
+def run_dense(args, rank, world):
+    """Dense class: the complete graph K_n (every 16x128 tile full, so every tile takes the
+    binary tensor-core path), counted at tau = 0.  Reports the binary MMA throughput of the
+    count against this GPU's measured b1 MMA peak (btc_b1_mma_peak)."""
+    import ctypes as C
+
+    import torch
+    from btc_b200 import BitBSR, graphs as G
+    from btc_b200._lib import lib
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    n = args.n_dense
+    s_, d_, _ = G.complete(n)
+    g = BitBSR(torch.from_numpy(s_).cuda(), torch.from_numpy(d_).cuda(), n, 128)
+    want = n * (n - 1) * (n - 2) // 6
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    for _ in range(args.warmup):
+        assert g.count(tau=0) == want
+    ts = []
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            c, ms = g.count(tau=0, timing=True)
+            assert c == want
+            ts.append(ms)
+    t = statistics.median(ts) / 1e3
+    triples = dense_triples(g.to_host(), 128, 0)
+    ops = triples * 16 * 16 * 128
+    peak = C.c_double(0.0)
+    lib().btc_b1_mma_peak(None, 4000, C.byref(peak))
+    m_lower = n * (n - 1) // 2
+    line = {
+        "metric": METRIC, "value": m_lower / t, "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "b1",
+        "data": "synthetic",
+        "config": {"workload": f"complete graph K_{n} (dense class), count only, tau = 0",
+                   "edges": m_lower, "tiles": g.num_tiles, "tile": "16x128",
+                   "l2": "flushed before every timed count (512 MB write)"},
+        "tensor": {"triples": triples, "ops_b1": ops, "achieved_tops": ops / t / 1e12,
+                   "peak_tops": peak.value / 1e12, "frac": ops / t / peak.value,
+                   "peak_source": "btc_b1_mma_peak (mma.sync m16n8k128 b1 and.popc, this GPU)"},
+        "clocks": clk.summary(),
+    }
+    g.free()
+    print(json.dumps(line), flush=True)
+
+
 def run_batch(args, rank, world):
     """Batched workload: many graphs in one build + one count launch, against the plain
     path (one build + one count + one host sync per graph, reusing one handle)."""
@@ -432,6 +507,7 @@ def main():
     ap.add_argument("--requests", type=int, default=2000, help="serve workload: requests per rate")
     ap.add_argument("--rates", default="50,200,1000,5000", help="serve workload: arrivals/s")
     ap.add_argument("--large-frac", type=float, default=0.05, help="serve workload: large share")
+    ap.add_argument("--n-dense", type=int, default=4096, help="dense workload: K_n vertices")
     ap.add_argument("--shard", action="store_true",
                     help="one graph per job: every rank counts a cost-balanced tile range of the "
                          "same Bit-BSR and the counts are all-reduced (strong scaling); default: "
@@ -451,6 +527,10 @@ def main():
         return
     if args.workload == "serve":
         run_serve(args, rank, world)
+        return
+    if args.workload == "dense":
+        if rank == 0:
+            run_dense(args, rank, world)
         return
 
     import torch

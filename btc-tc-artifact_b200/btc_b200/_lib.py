@@ -62,6 +62,7 @@ EXPORTS = [
     "btc_partition_tiles",
     "btc_partition_from_costs",
     "btc_count_tiles_async",
+    "btc_b1_mma_peak",
 ]
 
 
@@ -175,6 +176,7 @@ def lib():
         L.btc_partition_tiles.argtypes = [vp, C.c_int, vp, vp]
         L.btc_partition_from_costs.argtypes = [vp, C.c_uint64, u32, u32, C.c_int, vp]
         L.btc_count_tiles_async.argtypes = [vp, u32, u32, C.c_int, vp, vp]
+        L.btc_b1_mma_peak.argtypes = [vp, C.c_int, C.POINTER(C.c_double)]
         for name in EXPORTS:
             if name not in ("btc_bcsr_free", "btc_free", "btc_strerror", "btc_batch_free",
                             "btc_server_default_config", "btc_server_destroy"):

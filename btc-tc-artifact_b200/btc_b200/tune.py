@@ -8,6 +8,10 @@ on the standard graphs and prints a markdown table (microseconds per launch).
 
 ``tune.py --count GRAPH --tile C [--reps K]`` builds one standard graph and counts it K
 times (default tau), printing the counts: a fixed target for profilers.
+
+``autotune(src, dst, n)`` measures the tile width for one graph (both widths built and
+timed, counts cross-checked); ``tune.py --autotune`` prints it for the standard graphs
+next to the reference's BTC-Lite choice.
 """
 from __future__ import annotations
 
@@ -32,6 +36,48 @@ def tau_sweep(g, taus=TAUS, reps: int = 30) -> dict:
             times.append(ms)
         out[tau] = statistics.median(times)
     return out
+
+
+def autotune(src, dst, n: int, orient_degree: bool = False, tiles=(32, 128), reps: int = 5,
+             stream=None) -> dict:
+    """Measured tile-width choice for one graph (the reference's tile policy is the fixed
+    BTC-Lite rule, apps/btc_tc_lite.cu:45-65).  Builds the Bit-BSR at every width in
+    `tiles`, times rebuild and count (CUDA events, medians of `reps`), checks that all
+    widths give the same count, and returns {"tile_cols": best by build + count,
+    "count": c, "lite_policy": the BTC-Lite choice, "table": {C: {"build_ms", "count_ms",
+    "tiles"}}}."""
+    import torch
+
+    from . import _lib
+    from .api import BitBSR
+
+    def ms_of(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        st = torch.cuda.current_stream() if stream is None else stream
+        e0.record(st)
+        fn()
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    table, count = {}, None
+    for C in tiles:
+        g = BitBSR(src, dst, n, C, orient_degree=orient_degree, stream=stream)
+        c = g.count(stream=stream)
+        if count is None:
+            count = c
+        if c != count:
+            raise AssertionError(f"16x{C} counted {c}, the first width {count}")
+        builds = [ms_of(lambda: g.rebuild(src, dst, n, C, orient_degree=orient_degree,
+                                          stream=stream)) for _ in range(reps)]
+        counts = [g.count(stream=stream, timing=True)[1] for _ in range(reps)]
+        table[C] = {"build_ms": statistics.median(builds), "count_ms": statistics.median(counts),
+                    "tiles": g.num_tiles}
+        g.free()
+    m = int(src.numel()) if hasattr(src, "numel") else len(src)
+    best = min(table, key=lambda C: table[C]["build_ms"] + table[C]["count_ms"])
+    lite = int(_lib.lib().btc_lite_select_tile_cols(m, int(n), 0))
+    return {"tile_cols": best, "count": count, "lite_policy": lite, "table": table}
 
 
 def standard_graphs(names=None):
@@ -65,9 +111,23 @@ def main() -> None:
     ap.add_argument("--count", default=None, help="count one standard graph instead of the sweep")
     ap.add_argument("--tile", type=int, default=128)
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--autotune", action="store_true",
+                    help="measured tile width per standard graph against the BTC-Lite rule")
     args = ap.parse_args()
     if args.count:
         count_once(args.count, args.tile, args.reps)
+        return
+    if args.autotune:
+        print("| graph | BTC-Lite | measured best | 16x32 build+count ms | 16x128 build+count ms |")
+        print("|---|---|---|---|---|")
+        for name, (s_, d_, n_), deg in standard_graphs(["stencil27_64", "er_16384_16",
+                                                        "rmat18_deg", "rmat20_deg"]):
+            r = autotune(torch.from_numpy(s_).cuda(), torch.from_numpy(d_).cuda(), n_,
+                         orient_degree=deg)
+            t = r["table"]
+            print(f"| {name} | 16x{r['lite_policy']} | 16x{r['tile_cols']} | "
+                  f"{t[32]['build_ms']:.3f} + {t[32]['count_ms']:.3f} | "
+                  f"{t[128]['build_ms']:.3f} + {t[128]['count_ms']:.3f} |", flush=True)
         return
     print("| graph | tile | tiles | " + " | ".join(
         "all-sparse" if t == 0x7FFFFFFF else f"tau={t}" for t in TAUS) + " |")

@@ -220,6 +220,12 @@ BTC_API int btc_partition_from_costs(const unsigned long long* bucket_cost, uint
 BTC_API int btc_count_tiles_async(btc_bitbsr* g, uint32_t tile_begin, uint32_t tile_end, int tau,
                                   btc_stream_t stream, unsigned long long* d_out);
 
+/* Diagnostic (no counterpart in the reference): binary AND-popcount-accumulates per
+ * second of mma.sync.m16n8k128...b1.and.popc on this GPU (the dense path's instruction),
+ * measured with `iters` rounds of independent MMAs per warp on a persistent grid; the
+ * denominator of the dense class's tensor-core utilisation. */
+BTC_API int btc_b1_mma_peak(btc_stream_t stream, int iters, double* ops_per_s);
+
 /* Fills *v with the handle's arrays and sizes. */
 BTC_API int btc_bitbsr_info(const btc_bitbsr* g, btc_bitbsr_view* v);
 
