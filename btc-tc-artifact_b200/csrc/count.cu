@@ -377,10 +377,12 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
     // Tile queue over one word.  Grab k is a run of consecutive tiles.  When no row
     // block holds more than four times the mean number of tiles plus 8 (meshes,
     // Erdos-Renyi: tile costs alike), the schedule is guided: `chunk` tiles in the first
-    // grid-wide round of grabs, half as many in each later round, down to single tiles.
+    // grid-wide round of grabs, half as many in each later round, down to two tiles.
     // Otherwise (power-law graphs, where a run of tiles can cost many times another) every
-    // grab is `chunk_skewed` tiles.  A warp asks for its next grab while it counts the
-    // last tile of the current one, so it never holds more than one grab.
+    // grab is `chunk_skewed` tiles.  Grab k < (warps in the grid) is warp k's first grab;
+    // later grabs are numbered by an atomic on the queue word.  A warp asks for its next
+    // grab while it counts the last tile of the current one, so it never holds more than
+    // one grab.
     const unsigned long long nwarps = (unsigned long long)gridDim.x * kWarps;
     bool guided = false;
     if (row_max) {
@@ -391,7 +393,7 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
     auto grab_range = [&](unsigned long long k, uint32_t& b, uint32_t& e) {
         unsigned long long off = 0;
         uint32_t sz = chunk;
-        while (guided && sz > 1 && k >= nwarps) {
+        while (guided && sz > 2 && k >= nwarps) {
             off += nwarps * sz;
             k -= nwarps;
             sz >>= 1;
@@ -430,8 +432,10 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
     uint32_t t, ce;  // current tile and the end of its grab
     {
         unsigned long long k = 0;
-        if (lane == 0) k = atomicAdd(scr.work, 1ull);
-        grab_range(__shfl_sync(kFull, k, 0), t, ce);
+        // the first grab of every warp is its own index (no atomic at launch); the queue
+        // word numbers the later grabs
+        k = (unsigned long long)blockIdx.x * kWarps + warp;
+        grab_range(k, t, ce);
     }
     uint32_t I = 0, JL = 0, w0 = 0, w1 = 0, ptrs = 0;
     if (t < tile_end) {
@@ -452,7 +456,7 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
             load_ids(tn, nI, nJL, nw0, nw1);
             nstate = 0;
         } else {
-            if (lane == 0) kq = atomicAdd(scr.work, 1ull);
+            if (lane == 0) kq = nwarps + atomicAdd(scr.work, 1ull);
             nstate = 2;
         }
         auto next_ready = [&]() {
@@ -824,12 +828,13 @@ int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
     const uint32_t span = build_meta ? min(tiles_hint, tile_end - tile_begin) : tile_end - tile_begin;
     const int grid = count_grid_size(tile_cols);
     // Guided schedule: the first round of grabs is about half of an even share per warp
-    // (1 to 64 tiles).  Fixed schedule: about an eighth of an even share (8 to 64 tiles);
+    // (2 to 64 tiles; later rounds halve it down to 2: a one-tile grab costs a contended
+    // queue atomic per tile).  Fixed schedule: about an eighth of an even share (8 to 64 tiles);
     // a grab of a power-law graph's row block often holds tiles of one long list, which
     // is staged once per grab.
     const uint64_t warps = (uint64_t)grid * kWarps;
     uint64_t chunk = span / (warps * 2), chunk_s = span / (warps * 8);
-    chunk = chunk < 1 ? 1 : (chunk > 64 ? 64 : chunk);
+    chunk = chunk < 2 ? 2 : (chunk > 64 ? 64 : chunk);
     chunk_s = chunk_s < 8 ? 8 : (chunk_s > 64 ? 64 : chunk_s);
     // The occupancy masks and the two-direction search pay off only where row blocks
     // hold many tiles (long lists to search); meshes and stencils (a few tiles per row
