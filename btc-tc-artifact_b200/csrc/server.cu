@@ -12,8 +12,11 @@
 // completes; every result carries the request's submit and completion times on the
 // server's steady clock.  A request of at least solo_edges edges runs alone on a slot
 // through the single-graph path with descending-degree orientation (batching gains
-// nothing for it, and degree order keeps its hub rows short).  With slots = 1 and
-// max_batch_graphs = 1 the same server is the plain one-request-at-a-time path.
+// nothing for it, and degree order keeps its hub rows short) once it reaches the front
+// of the queue; a batch being formed passes over such requests and takes the small ones
+// behind them.  Solo rebuilds are enqueued without a host wait, so the engine thread
+// keeps filling the other slots meanwhile.  With slots = 1 and max_batch_graphs = 1 the
+// same server is the plain one-request-at-a-time path.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -83,6 +86,7 @@ struct Slot {
     std::vector<int32_t> nv;
     size_t device_bytes = 0;
     bool busy = false;
+    bool solo_async = false;  // the solo handle's rebuild was enqueued without a wait
 };
 
 }  // namespace
@@ -202,12 +206,16 @@ int launch_slot(btc_server* s, Slot& sl)
     if (solo) {
         // a large graph gains nothing from batching; descending-degree orientation keeps
         // its hub rows short (BTC-Lite picks the tile width)
-        if (!sl.solo)
+        // Rebuilds are enqueued without a host wait (BTC_BUILD_ASYNC), so the engine
+        // thread goes on filling the other slots; finish_solo checks the build's status.
+        if (!sl.solo) {
             st = btc_build_bitbsr(ds, dd, m, sl.reqs[0].n, 0, BTC_ORIENT_DEGREE, sl.stream,
                                   &sl.solo);
-        else
-            st = btc_rebuild_bitbsr(sl.solo, ds, dd, m, sl.reqs[0].n, 0, BTC_ORIENT_DEGREE,
-                                    sl.stream);
+        } else {
+            st = btc_rebuild_bitbsr(sl.solo, ds, dd, m, sl.reqs[0].n, 0,
+                                    BTC_ORIENT_DEGREE | BTC_BUILD_ASYNC, sl.stream);
+            sl.solo_async = st == BTC_OK;
+        }
         if (st != BTC_OK) return st;
         st = btc_count_async(sl.solo, s->cfg.tau, sl.stream, sl.d_counts.as<unsigned long long>());
         if (st != BTC_OK) return st;
@@ -237,13 +245,36 @@ int launch_slot(btc_server* s, Slot& sl)
     return BTC_OK;
 }
 
+// Status of a finished slot whose solo graph was rebuilt without a wait: an enqueued
+// build that found more tiles than the handle's arrays hold built nothing, so it is
+// redone here with a waiting rebuild from the slot's device copy of the edges.
+int finish_solo(Slot& sl)
+{
+    if (!sl.solo_async) return BTC_OK;
+    sl.solo_async = false;
+    int st = resolve_build(sl.solo);
+    if (st != BTC_E_CAPACITY) return st;
+    const int64_t m = sl.offsets.back();
+    st = btc_rebuild_bitbsr(sl.solo, sl.d_src.as<int32_t>(), sl.d_dst.as<int32_t>(), m,
+                            sl.reqs[0].n, 0, BTC_ORIENT_DEGREE, sl.stream);
+    if (st == BTC_OK)
+        st = btc_count_async(sl.solo, BTC_TAU_DEFAULT, sl.stream,
+                             sl.d_counts.as<unsigned long long>());
+    if (st == BTC_OK &&
+        (cudaMemcpyAsync(sl.h_counts.p, sl.d_counts.ptr, sizeof(unsigned long long),
+                         cudaMemcpyDeviceToHost, sl.stream) != cudaSuccess ||
+         cudaStreamSynchronize(sl.stream) != cudaSuccess))
+        st = BTC_E_CUDA;
+    return st;
+}
+
 void engine_loop(btc_server* s)
 {
     cudaSetDevice(s->device);
     for (;;) {
         // 1. publish finished slots
         for (Slot& sl : s->slots)
-            if (sl.busy && cudaEventQuery(sl.done) == cudaSuccess) publish(s, sl, BTC_OK);
+            if (sl.busy && cudaEventQuery(sl.done) == cudaSuccess) publish(s, sl, finish_solo(sl));
 
         // 2. fill a free slot from the queue
         Slot* free_slot = nullptr;
@@ -274,11 +305,20 @@ void engine_loop(btc_server* s)
                 sl.nv.clear();
                 int64_t m = 0, rows = 0;
                 const int tile = s->cfg.tile_cols ? s->cfg.tile_cols : 128;
-                while (!s->pending.empty() && (int)sl.reqs.size() < s->cfg.max_batch_graphs) {
-                    Request& q = s->pending.front();
+                // A batch under way passes over large requests (they run alone when they
+                // reach the front), looking at most this many queued requests.
+                const size_t max_scan = 4 * (size_t)s->cfg.max_batch_graphs + 64;
+                size_t scanned = 0;
+                auto it = s->pending.begin();
+                while (it != s->pending.end() && (int)sl.reqs.size() < s->cfg.max_batch_graphs &&
+                       scanned++ < max_scan) {
+                    Request& q = *it;
                     const int64_t qm = q.m;
                     // a large request runs alone (solo path)
-                    if (!sl.reqs.empty() && qm >= s->cfg.solo_edges) break;
+                    if (!sl.reqs.empty() && qm >= s->cfg.solo_edges) {
+                        ++it;
+                        continue;
+                    }
                     const int64_t qr = ((int64_t)q.n + 15) / 16;
                     const size_t need = batch_bytes_bound(m + qm, rows + qr, tile);
                     if (!sl.reqs.empty() &&
@@ -294,7 +334,7 @@ void engine_loop(btc_server* s)
                         r.submit_s = q.submit_s;
                         r.done_s = s->now();
                         rejected.push_back(r);
-                        s->pending.pop_front();
+                        it = s->pending.erase(it);
                         continue;
                     }
                     if (sl.reqs.empty() && batch_bytes_bound(qm, qr, tile) > budget) break;
@@ -303,7 +343,7 @@ void engine_loop(btc_server* s)
                     sl.reqs.push_back(std::move(q));
                     sl.offsets.push_back(m);
                     sl.nv.push_back(sl.reqs.back().n);
-                    s->pending.pop_front();
+                    it = s->pending.erase(it);
                     if (qm >= s->cfg.solo_edges) break;
                 }
                 if (!rejected.empty()) {
