@@ -49,6 +49,7 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / kWarp;
 constexpr int kACap = 256;     // list mode: row-block list entries staged per warp
+constexpr int kSmallList = 16; // lists this short are staged as lists, not bitmaps
 constexpr int kBmWords = 256;  // bitmap mode: graphs with at most 8192 column blocks
 constexpr int kMCap = 64;      // matches buffered per warp before a bit pass
 constexpr int kBCap = 512;     // mask-bit codes buffered per warp per bit pass
@@ -146,7 +147,12 @@ __device__ __forceinline__ ARow stage_row(WarpSmem<C>& s, const uint32_t* __rest
     A.last = indices[A.start + A.len - 1];
     A.words = ((A.last - A.base) >> 5) + 1;
     __syncwarp();  // earlier readers of s.a / s.apre are done
-    if (A.words <= (uint32_t)kBmWords) {
+    if (A.len <= (uint32_t)kSmallList) {
+        // a short list (meshes: a few tiles per row block) is staged as it is, one element
+        // per lane, and searched by bisection: cheaper than building a bitmap per tile run
+        A.mode = 0;
+        if ((uint32_t)lane < A.len) s.a.list[lane] = indices[A.start + lane];
+    } else if (A.words <= (uint32_t)kBmWords) {
         A.mode = 1;
         for (uint32_t w = lane; w < A.words; w += kWarp) s.a.bm[w] = 0u;
         __syncwarp();
