@@ -248,7 +248,7 @@ int launch_slot(btc_server* s, Slot& sl)
 // Status of a finished slot whose solo graph was rebuilt without a wait: an enqueued
 // build that found more tiles than the handle's arrays hold built nothing, so it is
 // redone here with a waiting rebuild from the slot's device copy of the edges.
-int finish_solo(Slot& sl)
+int finish_solo(Slot& sl, int tau)
 {
     if (!sl.solo_async) return BTC_OK;
     sl.solo_async = false;
@@ -258,8 +258,7 @@ int finish_solo(Slot& sl)
     st = btc_rebuild_bitbsr(sl.solo, sl.d_src.as<int32_t>(), sl.d_dst.as<int32_t>(), m,
                             sl.reqs[0].n, 0, BTC_ORIENT_DEGREE, sl.stream);
     if (st == BTC_OK)
-        st = btc_count_async(sl.solo, BTC_TAU_DEFAULT, sl.stream,
-                             sl.d_counts.as<unsigned long long>());
+        st = btc_count_async(sl.solo, tau, sl.stream, sl.d_counts.as<unsigned long long>());
     if (st == BTC_OK &&
         (cudaMemcpyAsync(sl.h_counts.p, sl.d_counts.ptr, sizeof(unsigned long long),
                          cudaMemcpyDeviceToHost, sl.stream) != cudaSuccess ||
@@ -274,7 +273,7 @@ void engine_loop(btc_server* s)
     for (;;) {
         // 1. publish finished slots
         for (Slot& sl : s->slots)
-            if (sl.busy && cudaEventQuery(sl.done) == cudaSuccess) publish(s, sl, finish_solo(sl));
+            if (sl.busy && cudaEventQuery(sl.done) == cudaSuccess) publish(s, sl, finish_solo(sl, s->cfg.tau));
 
         // 2. fill a free slot from the queue
         Slot* free_slot = nullptr;
