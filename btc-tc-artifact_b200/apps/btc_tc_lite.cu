@@ -7,7 +7,9 @@
 //   btc_tc_lite -i graph.bin [-w warmup] [-r repeat]     (BTC_MODE=0|1|2)
 //
 // Input: the reference's binary CSR (btc/utils/io/read.h:255-299: int32 nrow, ncol,
-// nnz; int32 row_ptr[nrow+1]; int32 col[nnz]; float val[nnz]) or a text edge list
+// nnz; int32 row_ptr[nrow+1]; int32 col[nnz]; float val[nnz]), a Matrix Market
+// coordinate file (".mtx", the format read.h:33-189 reads: 1-based "i j [value]" entries
+// after the banner, comments and the size line; values are ignored) or a text edge list
 // (".el": "u v" per line).
 #include <algorithm>
 #include <cstdio>
@@ -73,6 +75,48 @@ bool read_el(const char* path, std::vector<int>& rows, std::vector<int>& cols, i
     return true;
 }
 
+bool ends_with(const std::string& s, const char* suffix)
+{
+    const size_t k = std::strlen(suffix);
+    return s.size() >= k && s.compare(s.size() - k, k, suffix) == 0;
+}
+
+// Matrix Market coordinate file: banner "%%MatrixMarket matrix coordinate <field>
+// <symmetry>", '%' comment lines, "rows cols entries", then one "i j [value...]" line per
+// entry with 1-based i, j.  Only the pattern matters here (the count orients and
+// deduplicates the edges), so values and the symmetry flag are not needed.
+bool read_mtx(const char* path, std::vector<int>& rows, std::vector<int>& cols, int& n)
+{
+    FILE* f = std::fopen(path, "r");
+    if (!f) return false;
+    char line[1024];
+    bool ok = std::fgets(line, sizeof line, f) != nullptr &&
+              std::strncmp(line, "%%MatrixMarket", 14) == 0 && std::strstr(line, "coordinate");
+    long long nr = 0, nc = 0, nnz = 0;
+    while (ok) {  // comments, then the size line
+        if (!std::fgets(line, sizeof line, f)) {
+            ok = false;
+            break;
+        }
+        if (line[0] == '%') continue;
+        ok = std::sscanf(line, "%lld %lld %lld", &nr, &nc, &nnz) == 3 && nr >= 0 && nc >= 0 &&
+             nnz >= 0 && nr <= 0x7fffffff && nc <= 0x7fffffff;
+        break;
+    }
+    for (long long e = 0; ok && e < nnz; ++e) {
+        long long i, j;
+        ok = std::fgets(line, sizeof line, f) != nullptr &&
+             std::sscanf(line, "%lld %lld", &i, &j) == 2 && i >= 1 && j >= 1 && i <= nr && j <= nc;
+        if (ok) {
+            rows.push_back((int)(i - 1));
+            cols.push_back((int)(j - 1));
+        }
+    }
+    std::fclose(f);
+    n = (int)std::max(nr, nc);
+    return ok;
+}
+
 }  // namespace
 
 int main(int argc, char** argv)
@@ -94,9 +138,9 @@ int main(int argc, char** argv)
     std::vector<int> hrows, hcols;
     int n = 0;
     const std::string path(input);
-    const bool ok = path.size() > 3 && path.compare(path.size() - 3, 3, ".el") == 0
-                        ? read_el(input, hrows, hcols, n)
-                        : read_bin(input, hrows, hcols, n);
+    const bool ok = ends_with(path, ".el")    ? read_el(input, hrows, hcols, n)
+                    : ends_with(path, ".mtx") ? read_mtx(input, hrows, hcols, n)
+                                              : read_bin(input, hrows, hcols, n);
     if (!ok) {
         std::printf("cannot read %s\n", input);
         return 1;

@@ -176,6 +176,17 @@ def write_bin_csr(path: str, rowptr, col, n: int):
         np.ones(len(col), np.float32).tofile(f)
 
 
+def write_mtx(path: str, src, dst, n: int):
+    """Write an edge list as a Matrix Market coordinate pattern file (the format the
+    reference reads in btc/utils/io/read.h:33-189): each undirected edge once, in the lower
+    triangle (row > col), 1-based, self-loops and duplicates removed."""
+    r, c = lower_coo(src, dst, n)
+    with open(path, "w") as f:
+        f.write("%%MatrixMarket matrix coordinate pattern symmetric\n")
+        f.write(f"{n} {n} {len(r)}\n")
+        np.savetxt(f, np.stack([r + 1, c + 1], axis=1), fmt="%d")
+
+
 def union_graph(graphs):
     """Block-diagonal union of graphs, laid out as a batch lays them out: graph g's
     vertex v becomes 16 * (row blocks of graphs before g) + v."""

@@ -414,6 +414,24 @@ def test_rmat_scale18_orders_and_paths_agree():
     assert counts == {want}
 
 
+@pytest.mark.parametrize("name", ["stencil27_16", "rmat_12_16_s7", "K130", "stencil7_8"])
+def test_compat_cli_reads_matrix_market(name, tmp_path):
+    """apps/btc_tc_lite.cu reads a Matrix Market coordinate file (graphs.write_mtx)."""
+    import os
+    import re
+    import subprocess
+    fx = load_golden()[name]
+    src, dst, n = golden_graph(name)
+    path = tmp_path / f"{name}.mtx"
+    G.write_mtx(str(path), src, dst, n)
+    app = os.path.join(os.path.dirname(_lib.LIB_PATH), "btc_tc_lite")
+    out = subprocess.run([app, "-i", str(path), "-w", "1", "-r", "2"], capture_output=True,
+                         text=True, timeout=120)
+    assert out.returncode == 0, out.stdout + out.stderr
+    got = int(re.search(r"Triangles \(GPU\): (\d+)", out.stdout).group(1))
+    assert got == fx["count"], out.stdout
+
+
 @pytest.mark.parametrize("name", ["stencil27_16", "rmat_12_16_s7", "K130"])
 def test_compat_cli_reads_reference_bin_format(name, tmp_path):
     """apps/btc_tc_lite.cu: the reference's CLI flow over btc_compat.hpp, fed the

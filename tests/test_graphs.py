@@ -62,3 +62,19 @@ def test_lower_coo_and_bin_writer(tmp_path):
     assert raw[:3].tolist() == [4, 4, 3]
     assert raw[3:8].tolist() == rowptr.tolist()
     assert raw[8:11].tolist() == c.tolist()
+
+
+def test_write_mtx_is_lower_triangle_pattern(tmp_path):
+    import numpy as np
+    from btc_b200 import graphs as G
+    s, d, n = G.stencil27(4)
+    p = tmp_path / "g.mtx"
+    G.write_mtx(str(p), s, d, n)
+    lines = p.read_text().splitlines()
+    assert lines[0] == "%%MatrixMarket matrix coordinate pattern symmetric"
+    nr, nc, nnz = map(int, lines[1].split())
+    assert nr == nc == n and nnz == len(lines) - 2
+    e = np.array([list(map(int, ln.split())) for ln in lines[2:]])
+    assert (e[:, 0] > e[:, 1]).all() and e.min() >= 1 and e.max() <= n
+    r, c = G.lower_coo(s, d, n)
+    assert nnz == len(r) and len({(a, b) for a, b in e}) == nnz
