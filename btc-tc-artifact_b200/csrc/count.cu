@@ -518,12 +518,14 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
         if (lane <= JPT) s.jptr[lane] = ptrs;
         __syncwarp();
 
-        // unit prefix over active slices
+        // unit prefix over active slices (the search's lane -> slice map)
         uint32_t upre[JPT + 1];
-        upre[0] = 0;
+        auto compute_upre = [&]() {
+            upre[0] = 0;
 #pragma unroll
-        for (int j = 0; j < JPT; ++j)
-            upre[j + 1] = upre[j] + (((active >> j) & 1u) ? (s.jptr[j + 1] - s.jptr[j]) : 0u);
+            for (int j = 0; j < JPT; ++j)
+                upre[j + 1] = upre[j] + (((active >> j) & 1u) ? (s.jptr[j + 1] - s.jptr[j]) : 0u);
+        };
 
         if (nnz <= tau) {
             // ================= sparse path ===================================
@@ -540,6 +542,7 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
             e -= mine;
             const uint32_t* __restrict__ rmask_g = nullptr;
             if constexpr (kHeavy) {
+                compute_upre();
                 // Tiles with more than one round of list elements take the heavy path:
                 // rows and columns of S that carry bits, per slice (to drop matches and
                 // units whose tile rows are empty), and the two-direction search plan.
@@ -596,6 +599,40 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
                     }
                 }
             }
+            bool searched = false;
+            if constexpr (!kHeavy) {
+                // When every active slice's list fits in its share of the lanes (meshes:
+                // a few column blocks per row block), one round with a fixed lane -> slice
+                // map does the search; the ballot order keeps matches grouped by slice.
+                constexpr int LPS = kWarp / JPT;  // lanes per slice
+                const int jl = lane / LPS, ql = lane % LPS;
+                const uint32_t jb = __shfl_sync(kFull, ptrs, jl);
+                const uint32_t je = __shfl_sync(kFull, ptrs, jl + 1);
+                const uint32_t len = ((active >> jl) & 1u) ? je - jb : 0u;
+                if (__all_sync(kFull, len <= (uint32_t)LPS)) {
+                    bool found = false;
+                    uint32_t pa = 0;
+                    const uint32_t pb = jb + (uint32_t)ql;
+                    if ((uint32_t)ql < len) found = a_lookup<C>(s, A, indices, indices[pb], pa);
+                    const unsigned mb = __ballot_sync(kFull, found);
+                    if (found) {
+                        const uint32_t k = __popc(mb & lt);
+                        s.mpa[k] = pa;
+                        s.mpb[k] = pb;
+                    }
+                    if (lane <= JPT)
+                        s.mc[lane] = __popc(mb & (lane == JPT ? kFull : ((1u << (lane * LPS)) - 1u)));
+                    next_ready();
+                    __syncwarp();
+                    if (mb)
+                        acc += bit_pass<C, kHeavy>(s, w0, w1, e, (uint32_t)nnz, 0u,
+                                                   (uint32_t)__popc(mb), blocks, lane);
+                    searched = true;
+                } else {
+                    compute_upre();
+                }
+            }
+            if (!searched) {
             if (lane == 0) {
 #pragma unroll
                 for (int j = 0; j <= JPT; ++j) s.upre[j] = upre[j];
@@ -664,6 +701,7 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
                     acc += bit_pass<C, kHeavy>(s, w0, w1, e, (uint32_t)nnz, lo, nm, blocks, lane);
                     lo = nm;
                 }
+            }
             }
         } else {
             // ================= dense path: binary tensor core ================
