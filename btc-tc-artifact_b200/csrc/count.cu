@@ -40,6 +40,8 @@
 //    pack four matches into the 128-bit k dimension, as tc_16x32_mma_v6.h:72-154 does.
 #include "common.cuh"
 
+#include <cstddef>
+
 #include <atomic>
 
 namespace btc200 {
@@ -64,6 +66,8 @@ struct Cfg {
 template <int C>
 struct __align__(16) WarpSmem {
     uint32_t S[Cfg<C>::TW];          // sample tile (dense path)
+    uint32_t nS[Cfg<C>::TW];         // the next tile's sample words (cp.async prefetch; 8-byte
+                                     // copies, so it sits at a 16-byte-aligned offset)
     union {
         uint32_t list[kACap];        // row block I's column blocks (list mode)
         uint32_t bm[kBmWords];       // the same as a bitmap (bitmap mode)
@@ -82,6 +86,25 @@ struct __align__(16) WarpSmem {
     uint16_t cmask[Cfg<C>::JPT];     // columns (rows of J_out tiles) with bits in slice j
     uint16_t bits[kBCap];            // (row << 8) | column of the sample tile's set bits
 };
+static_assert(offsetof(WarpSmem<128>, nS) % 16 == 0 && offsetof(WarpSmem<32>, nS) % 16 == 0,
+              "cp.async destinations must be aligned to the copy size");
+static_assert(sizeof(WarpSmem<128>) % 16 == 0 && sizeof(WarpSmem<32>) % 16 == 0,
+              "per-warp areas keep the 16-byte alignment of the first one");
+
+// global -> shared copies that complete in the background (cp.async, sm_80+); the issuing
+// lane waits with cp_async_wait_all, then a __syncwarp publishes the words to the warp.
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // Row block I's column-block list as the search structure of the current tile.
 struct ARow {
@@ -422,6 +445,29 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
             x1 = 0u;
         }
     };
+    // The next tile's ids, and its sample words copied into s.nS in the background (no
+    // registers held across the current tile); next_words() reads them back.
+    auto load_next = [&](uint32_t t, uint32_t& tI, uint32_t& tJL) {
+        tI = row_indices[t];
+        tJL = indices[t];
+        if constexpr (C == 128) {
+            cp_async8(&s.nS[2 * lane], blocks + (size_t)t * TW + 2 * lane);
+        } else {
+            if (lane < 16) cp_async4(&s.nS[lane], blocks + (size_t)t * TW + lane);
+        }
+        cp_async_commit();
+    };
+    auto next_words = [&](uint32_t& x0, uint32_t& x1) {
+        cp_async_wait_all();
+        __syncwarp();
+        if constexpr (C == 128) {
+            x0 = s.nS[2 * lane];
+            x1 = s.nS[2 * lane + 1];
+        } else {
+            x0 = lane < 16 ? s.nS[lane] : 0u;
+            x1 = 0u;
+        }
+    };
     // A tile's indptr words: lane j <= JPT holds indptr[J_L*JPT + j] (the row blocks
     // J_out of its slices), lanes 16 and 17 hold indptr[I] and indptr[I + 1].
     auto load_ptrs = [&](uint32_t tI, uint32_t tJL) -> uint32_t {
@@ -453,13 +499,13 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
         // this tile's search has issued its loads; after the grab's last tile the queue
         // atomic is issued now and read once this tile's search is under way.
         uint32_t tn = t + 1, cen = ce;
-        uint32_t nI = 0, nJL = 0, nw0 = 0, nw1 = 0, nptrs = 0;
+        uint32_t nI = 0, nJL = 0, nptrs = 0;
         // 0: next ids loading; 1: and its indptr words; 2: queue atomic in flight;
         // 3: grab resolved, ids loading (indptr words loaded at the top of the next tile)
         int nstate;
         unsigned long long kq = 0;
         if (tn < ce) {
-            load_ids(tn, nI, nJL, nw0, nw1);
+            load_next(tn, nI, nJL);
             nstate = 0;
         } else {
             if (lane == 0) kq = nwarps + atomicAdd(scr.work, 1ull);
@@ -468,7 +514,7 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
         auto next_ready = [&]() {
             if (nstate == 2) {
                 grab_range(__shfl_sync(kFull, kq, 0), tn, cen);
-                if (tn < tile_end) load_ids(tn, nI, nJL, nw0, nw1);
+                if (tn < tile_end) load_next(tn, nI, nJL);
                 nstate = 3;
             } else if (nstate == 0 && !kHeavy) {
                 // (heavy tiles are long: holding the next tile's words across one costs
@@ -782,8 +828,7 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
         ce = cen;
         I = nI;
         JL = nJL;
-        w0 = nw0;
-        w1 = nw1;
+        if (t < tile_end) next_words(w0, w1);
         ptrs = nstate == 1 ? nptrs : (t < tile_end ? load_ptrs(I, JL) : 0u);
     }
 
