@@ -51,7 +51,7 @@ k_mark(const int32_t* __restrict__ src, const int32_t* __restrict__ dst, int64_t
        const int32_t* __restrict__ rank, uint64_t wpr, uint32_t* bitmap,
        unsigned long long* __restrict__ bad_count)
 {
-    constexpr int U = 4;  // edges in flight per thread
+    constexpr int U = 8;  // edges in flight per thread
     uint32_t nbad = 0;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < m; i0 += U * stride) {
@@ -288,7 +288,7 @@ k_fill_bm(const int32_t* __restrict__ src, const int32_t* __restrict__ dst, int6
     constexpr int C = 1 << LOG2C;
     constexpr int WPR = C / 32;
     constexpr int TW = 16 * WPR;
-    constexpr int U = 4;  // edges in flight per thread
+    constexpr int U = 8;  // edges in flight per thread
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < m; i0 += U * stride) {
         int32_t u[U], v[U];
@@ -355,7 +355,8 @@ __global__ void k_popcount_sum(const uint32_t* __restrict__ blocks, uint64_t wor
 int grid_for(int64_t work, int threads);
 int launch_tile_scan(uint32_t* per_tile, uint32_t ntiles, unsigned long long* total, cudaStream_t s);
 
-static int edge_grid(int64_t m) { return grid_for((m + 15) / 16, bm::kThreads); }
+// one round of U = 8 edges per thread (the grid is capped at 16 CTAs per SM)
+static int edge_grid(int64_t m) { return grid_for((m + 7) / 8, bm::kThreads); }
 
 uint64_t bitmap_words_per_row(const BuildGeom& g)
 {
