@@ -399,6 +399,29 @@ def test_config2_stencil_full_size():
     assert g.count(tau=0) == 11049696
 
 
+def test_host_input_full_size():
+    """The 64^3 stencil from pageable and from pinned host memory: the arrays equal the
+    device-input build's, asynchronous rebuilds from host memory keep the count, and an
+    out-of-range id in the last edge is still reported."""
+    src, dst, n = G.stencil27(64)
+    ref = BitBSR(_dev(src), _dev(dst), n, 128)
+    pinned = [torch.from_numpy(a).pin_memory().numpy() for a in (src, dst)]
+    for hs, hd in ((src, dst), pinned):
+        g = BitBSR(hs, hd, n, 128)
+        h, r = g.to_host(), ref.to_host()
+        for k in ("indptr", "indices", "row_indices", "blocks"):
+            assert np.array_equal(h[k], r[k]), k
+        for _ in range(3):
+            g.rebuild(hs, hd, n, 128, asynchronous=True)
+            assert g.count() == 11049696
+        g.free()
+    bad = src.copy()
+    bad[-1] = n
+    with pytest.raises(BtcError) as e:
+        BitBSR(bad, dst, n, 128)
+    assert e.value.status == _lib.BTC_E_RANGE
+
+
 def test_rmat_scale18_orders_and_paths_agree():
     src, dst, n = G.rmat(18, 16, seed=7)
     rp, col, _ = O.lower_csr(src, dst, n)
