@@ -201,6 +201,80 @@ def union_graph(graphs):
     return src, dst, base
 
 
+def batch_mix_plan(num_graphs: int, n_min: int = 256, n_max: int = 65536, seed: int = 0):
+    """The parameters of batch_mix's graphs without their edges: per graph (kind, n,
+    segments), a segment being (u_lo, u_hi, v_lo, v_hi, k) -- k pairs drawn uniformly from
+    [u_lo, u_hi) x [v_lo, v_hi) -- or, for R-MAT, ("rmat", scale, m).  Kinds, vertex counts,
+    degrees and R-MAT scales are batch_mix's (same seeds); the SBM block-pair edge counts
+    come from the same binomials, drawn in a different order."""
+    rng = np.random.default_rng(seed)
+    plan = []
+    for g in range(num_graphs):
+        gr = np.random.default_rng((seed, g))
+        kind = int(rng.integers(0, 3))
+        n = int(round(np.exp(rng.uniform(np.log(n_min), np.log(n_max)))))
+        if kind == 0:
+            d = rng.uniform(8, 32)
+            plan.append(("er", n, [(0, n, 0, n, int(round(n * d / 2)))]))
+        elif kind == 1:
+            p_in = rng.uniform(0.05, 0.3)
+            bounds = np.linspace(0, n, 9).astype(np.int64)
+            segs = []
+            for i in range(8):
+                for j in range(i, 8):
+                    ni, nj = bounds[i + 1] - bounds[i], bounds[j + 1] - bounds[j]
+                    pairs = ni * (ni - 1) // 2 if i == j else ni * nj
+                    k = int(gr.binomial(pairs, p_in if i == j else 0.001)) if pairs > 0 else 0
+                    if k:
+                        segs.append((int(bounds[i]), int(bounds[i + 1]), int(bounds[j]),
+                                     int(bounds[j + 1]), k))
+            plan.append(("sbm", n, segs))
+        else:
+            scale = int(rng.integers(10, 17))
+            plan.append(("rmat", 1 << scale, [("rmat", scale, 8 << scale)]))
+    return plan
+
+
+def batch_mix_device(num_graphs: int, n_min: int = 256, n_max: int = 65536, seed: int = 0,
+                     device="cuda"):
+    """batch_mix generated on the GPU: the same kinds, sizes and distributions (plan from
+    batch_mix_plan), the edges drawn by torch's seeded device generator (one per graph)
+    straight into two int32 device arrays, so batches of billions of edges need no host
+    memory.  Returns (src, dst, offsets int64[G+1], num_vertices int32[G], kinds)."""
+    import torch
+    plan = batch_mix_plan(num_graphs, n_min, n_max, seed)
+    sizes = [sum(sg[-1] for sg in segs) for _, _, segs in plan]
+    offsets = np.zeros(num_graphs + 1, np.int64)
+    offsets[1:] = np.cumsum(sizes)
+    src = torch.empty(int(offsets[-1]), dtype=torch.int32, device=device)
+    dst = torch.empty_like(src)
+    for g, (kind, n, segs) in enumerate(plan):
+        gen = torch.Generator(device=device)
+        gen.manual_seed(int(seed) * 1_000_003 + g)
+        a = int(offsets[g])
+        for sg in segs:
+            if sg[0] == "rmat":
+                _, scale, m = sg
+                u = torch.zeros(m, dtype=torch.int32, device=device)
+                v = torch.zeros_like(u)
+                for _ in range(scale):
+                    r = torch.rand(m, generator=gen, device=device)
+                    u = (u << 1) | (r >= 0.76).to(torch.int32)
+                    v = (v << 1) | (((r >= 0.57) & (r < 0.76)) | (r >= 0.95)).to(torch.int32)
+                src[a:a + m] = u
+                dst[a:a + m] = v
+                a += m
+                continue
+            u_lo, u_hi, v_lo, v_hi, k = sg
+            torch.randint(u_lo, u_hi, (k,), generator=gen, device=device, dtype=torch.int32,
+                          out=src[a:a + k])
+            torch.randint(v_lo, v_hi, (k,), generator=gen, device=device, dtype=torch.int32,
+                          out=dst[a:a + k])
+            a += k
+    nv = np.array([n for _, n, _ in plan], np.int32)
+    return src, dst, offsets, nv, [kind for kind, _, _ in plan]
+
+
 def batch_mix(num_graphs: int, n_min: int = 256, n_max: int = 65536, seed: int = 0):
     """The mixed batch workload: vertex counts log-uniform in [n_min, n_max]; each graph
     (seeded per graph) is Erdos-Renyi with mean degree U[8, 32], an 8-community SBM with

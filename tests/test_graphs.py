@@ -78,3 +78,30 @@ def test_write_mtx_is_lower_triangle_pattern(tmp_path):
     assert (e[:, 0] > e[:, 1]).all() and e.min() >= 1 and e.max() <= n
     r, c = G.lower_coo(s, d, n)
     assert nnz == len(r) and len({(a, b) for a, b in e}) == nnz
+
+
+def test_batch_mix_plan_matches_batch_mix():
+    """The plan behind the GPU-generated batch draws batch_mix's kinds, vertex counts and
+    ER / R-MAT sizes from the same seeds."""
+    host = G.batch_mix(48, 256, 65536, seed=3)
+    plan = G.batch_mix_plan(48, 256, 65536, seed=3)
+    for (s, d, n, kind), (pk, pn, segs) in zip(host, plan):
+        assert (kind, n) == (pk, pn)
+        if kind != "sbm":
+            assert len(s) == sum(sg[-1] for sg in segs)
+        else:
+            assert all(0 <= a < b <= n and 0 <= c < e <= n for a, b, c, e, _ in segs)
+
+
+def test_batch_mix_device_on_cpu_is_seeded_and_in_range():
+    torch = pytest.importorskip("torch")
+    a = G.batch_mix_device(24, 256, 4096, seed=5, device="cpu")
+    b = G.batch_mix_device(24, 256, 4096, seed=5, device="cpu")
+    src, dst, off, nv, kinds = a
+    assert torch.equal(src, b[0]) and torch.equal(dst, b[1])
+    assert off[0] == 0 and off[-1] == len(src) == len(dst) and len(nv) == len(kinds) == 24
+    for i in range(24):
+        s, d = src[off[i]:off[i + 1]], dst[off[i]:off[i + 1]]
+        if len(s):
+            assert int(s.min()) >= 0 and int(s.max()) < nv[i]
+            assert int(d.min()) >= 0 and int(d.max()) < nv[i]
