@@ -35,6 +35,9 @@ EXPORTS = [
     "btc_bcsr_reset_result",
     "btc_bcsr_get_result",
     "btc_preprocess_for_triangle_counting",
+    "btc_reorder_hashorder",
+    "btc_hashorder_params",
+    "btc_should_reorder",
     "btc_lite_select_tile_cols",
     "btc_build_bitbsr",
     "btc_rebuild_bitbsr",
@@ -144,6 +147,9 @@ def lib():
         L.btc_bcsr_reset_result.argtypes = [P(BtcBcsrDevice)]
         L.btc_bcsr_get_result.argtypes = [P(BtcBcsrDevice), P(C.c_ulonglong)]
         L.btc_preprocess_for_triangle_counting.argtypes = [vp, vp, P(C.c_int64), P(C.c_int32), C.c_int]
+        L.btc_reorder_hashorder.argtypes = [vp, vp, i64, i32, C.c_int, C.c_int, vp, vp]
+        L.btc_hashorder_params.argtypes = [C.c_int, vp, vp]
+        L.btc_should_reorder.argtypes = [i32, i64, C.c_int, C.c_char_p]
         L.btc_lite_select_tile_cols.argtypes = [i64, i32, C.c_int]
         L.btc_build_bitbsr.argtypes = [vp, vp, i64, i32, C.c_int, u32, vp, P(vp)]
         L.btc_rebuild_bitbsr.argtypes = [vp, vp, vp, i64, i32, C.c_int, u32, vp]

@@ -21,6 +21,8 @@ from __future__ import annotations
 
 import ctypes as C
 
+import os
+
 import numpy as np
 
 from . import _lib
@@ -79,10 +81,18 @@ class CooMatrix:
 
 def preprocess_for_triangle_counting(coo: CooMatrix, force_cpu: bool = False,
                                      lower_triangular: bool = True, input_file: str = "",
-                                     remap: bool = True) -> None:
-    """convert.h:600-612 with BTC_REORDER=0: orient to (max,min), drop self-loops,
-    sort, unique, and compact ids (remap).  Runs on the GPU whatever `force_cpu`
-    says (the engine has no CPU path); `lower_triangular=False` is not supported."""
+                                     remap: bool = True, reorder: int | None = None) -> None:
+    """convert.h:600-690: orient to (max,min), drop self-loops, sort, unique, compact ids
+    (remap), then the reorder step the reference selects with BTC_REORDER: 0 none, 8 GPU
+    HashOrder, 9 HashOrder when should_reorder_gpu says so (input_file's base name is
+    the dataset hint).  `reorder` overrides the environment; with neither, no reorder
+    (the reference defaults to 9: ids here stay stable unless asked).  Runs on the GPU
+    whatever `force_cpu` says (the engine has no CPU path); `lower_triangular=False` is
+    not supported."""
+    if reorder is None:
+        reorder = int(os.environ.get("BTC_REORDER", "0"))
+    if reorder not in (0, 8, 9):
+        raise BtcError(_lib.BTC_E_INVAL, f"reorder mode {reorder} (0, 8 and 9 are supported)")
     if not lower_triangular:
         raise BtcError(_lib.BTC_E_INVAL, "preprocess_for_triangle_counting(lower_triangular=False)")
     nnz = C.c_int64(coo.num_entries)
@@ -94,6 +104,45 @@ def preprocess_for_triangle_counting(coo: CooMatrix, force_cpu: bool = False,
     coo.row_indices = coo.row_indices[: nnz.value].clone()
     coo.column_indices = coo.column_indices[: nnz.value].clone()
     coo.num_rows = coo.num_cols = int(rows.value)
+    hint = os.path.splitext(os.path.basename(input_file))[0] if input_file else ""
+    if reorder == 8 or (reorder == 9 and should_reorder_gpu(coo, hint)):
+        reorder_hashorder_gpu(coo)
+
+
+def reorder_hashorder_gpu(coo: CooMatrix, num_hashes: int = 16, num_hops: int = 1):
+    """reorder.h:443-587 (btc_reorder_hashorder): relabels coo in place by MinHash
+    signature order and orients it to (max, min); returns the permutation as an int32
+    CUDA tensor (new id = perm[old id])."""
+    torch = _torch()
+    perm = torch.empty(max(coo.num_rows, 1), dtype=torch.int32, device=coo.row_indices.device)
+    check(lib().btc_reorder_hashorder(coo.row_indices.data_ptr(), coo.column_indices.data_ptr(),
+                                      int(coo.row_indices.numel()), int(coo.num_rows),
+                                      int(num_hashes), int(num_hops), perm.data_ptr(),
+                                      _stream_ptr(None)), "btc_reorder_hashorder")
+    return perm[: coo.num_rows]
+
+
+def hashorder_params(num_hashes: int = 16):
+    """The MinHash parameters (a, b) btc_reorder_hashorder uses, as uint32 arrays."""
+    a = np.zeros(num_hashes, np.uint32)
+    b = np.zeros(num_hashes, np.uint32)
+    check(lib().btc_hashorder_params(int(num_hashes), a.ctypes.data, b.ctypes.data),
+          "btc_hashorder_params")
+    return a, b
+
+
+def should_reorder(num_rows: int, nnz: int, sm_version: int, dataset_hint: str = "") -> bool:
+    """convert.h:443-596 (btc_should_reorder): the reference's automatic reorder rule."""
+    return bool(lib().btc_should_reorder(int(num_rows), int(nnz), int(sm_version),
+                                         dataset_hint.encode() if dataset_hint else None))
+
+
+def should_reorder_gpu(coo: CooMatrix, dataset_hint: str = "") -> bool:
+    """should_reorder_gpu (convert.h:579-596) for the current device."""
+    torch = _torch()
+    major, minor = torch.cuda.get_device_capability()
+    return should_reorder(coo.num_rows, int(coo.row_indices.numel()), 10 * major + minor,
+                          dataset_hint)
 
 
 class _BcsrDevice:

@@ -118,6 +118,32 @@ BTC_API int btc_bcsr_get_result(const btc_bcsr_device* bcsr, unsigned long long*
 BTC_API int btc_preprocess_for_triangle_counting(int32_t* d_rows, int32_t* d_cols, int64_t* nnz,
                                          int32_t* num_rows, int remap);
 
+/* Replaces btc::reorder_hashorder_gpu (btc/operations/reorder.h:443-587; BTC_REORDER=8, and
+ * what the default BTC_REORDER=9 runs when the automatic rule says so): relabels the
+ * vertices of a device COO in place so that vertices with similar neighbourhoods get
+ * nearby ids, then orients every entry to (max, min).  Signature of vertex v: num_hashes
+ * MinHash values over its num_hops-hop closed neighbourhood, h_j(v) = (a_j v + b_j) mod
+ * (2^32 - 5) with the reference's parameters (btc_hashorder_params); order: lexicographic
+ * by signature, ties by id.  The reference's defaults are num_hashes 16, num_hops 1.
+ * d_perm (nullable, num_rows int32) receives new id = d_perm[old id].  Ids outside
+ * [0, num_rows) give BTC_E_RANGE and leave the COO unchanged.  Allocates its workspace;
+ * blocking. */
+BTC_API int btc_reorder_hashorder(int32_t* d_rows, int32_t* d_cols, int64_t nnz, int32_t num_rows,
+                                  int num_hashes, int num_hops, int32_t* d_perm,
+                                  btc_stream_t stream);
+
+/* The hash parameters btc_reorder_hashorder uses (host only): a[j], b[j] for j <
+ * num_hashes (at most 64), drawn as reorder.h:495-506 draws them. */
+BTC_API int btc_hashorder_params(int num_hashes, uint32_t* a, uint32_t* b);
+
+/* Replaces btc::should_reorder_gpu (btc/operations/convert.h:579-596, with
+ * should_reorder_hopper_ampere 510-575 below sm_120 -- B200 is sm_100 -- and
+ * should_reorder_blackwell 443-505 from sm_120): whether the default preprocess reorders
+ * a graph of num_rows vertices and nnz COO entries.  dataset_hint (nullable) is the input
+ * file's base name.  Returns 1 or 0. */
+BTC_API int btc_should_reorder(int32_t num_rows, int64_t nnz, int sm_version,
+                               const char* dataset_hint);
+
 /* The BTC-Lite O(1) tile policy (apps/btc_tc_lite.cu:45-65): returns 32 or 128.
  * mode 1 forces 32, mode 2 forces 128 (the reference's BTC_MODE), 0 applies
  * "avg degree nnz/rows < 15 or rows < 50000 -> 32, else 128". */

@@ -10,7 +10,9 @@ checker, never the thing measured as the engine.
 * ``_ref/libref_cpu.so``: the reference's own ``cpu_tc_intersection_lower_triangular``
   (btc/operations/triangle_count_cpu.h:59-101) compiled from its header.
 * ``_ref/libref_gpu.so``: the reference's own Bit-BSR convert + adaptive count
-  kernels compiled for sm_100a (GPU only).
+  kernels and its GPU HashOrder (reorder.h:443-587), compiled for sm_100a (GPU only).
+* ``libhashparams.so`` (oracle/hashparams.cpp): the HashOrder hash parameters, drawn
+  with C++ <random> as reorder.h:495-506 draws them.
 """
 from __future__ import annotations
 
@@ -136,6 +138,57 @@ def density_hist(bsr):
 
 
 # ---------------------------------------------------------------------------
+# HashOrder (btc/operations/reorder.h:411-587), restated in numpy
+# ---------------------------------------------------------------------------
+_HASH_P = 4294967291  # the largest prime below 2^32 (reorder.h:415)
+_hashparams = None
+
+
+def hashorder_params(num_hashes: int = 16):
+    """(a, b) uint32 arrays drawn as reorder.h:495-506 draws them (oracle/hashparams.cpp)."""
+    global _hashparams
+    if _hashparams is None:
+        path = os.path.join(HERE, "libhashparams.so")
+        if not os.path.exists(path):
+            build(ref=False)
+        L = C.CDLL(path)
+        L.oracle_hashorder_params.restype = None
+        L.oracle_hashorder_params.argtypes = [C.c_int, _u32p, _u32p]
+        _hashparams = L
+    a = np.zeros(num_hashes, np.uint32)
+    b = np.zeros(num_hashes, np.uint32)
+    _hashparams.oracle_hashorder_params(int(num_hashes), a, b)
+    return a, b
+
+
+def hashorder(rows, cols, n: int, num_hashes: int = 16, num_hops: int = 1):
+    """reorder_hashorder_gpu (reorder.h:443-587) on a COO of n vertices: per hash j,
+    h_j(v) = (a_j v + b_j) mod P (411-418), num_hops rounds of
+    h(v) <- min(h(v), min over the neighbours u of h(u)) over the symmetric edge set
+    (421-441, 466-526), the vertices ordered lexicographically by (h_0, ..., h_{H-1}) with
+    ties by id (the stable LSD passes of 536-549), perm[order[i]] = i (556-563), both
+    endpoints relabelled and every entry oriented to (max, min) (569-584).
+    Returns (rows, cols, perm) as numpy arrays."""
+    rows = np.asarray(rows, np.int64)
+    cols = np.asarray(cols, np.int64)
+    a, b = hashorder_params(num_hashes)
+    v = np.arange(n, dtype=np.uint64)
+    h = (a.astype(np.uint64)[:, None] * v[None, :] + b.astype(np.uint64)[:, None]) % np.uint64(_HASH_P)
+    for _ in range(num_hops):
+        nxt = h.copy()
+        for j in range(num_hashes):
+            np.minimum.at(nxt[j], rows, h[j][cols])
+            np.minimum.at(nxt[j], cols, h[j][rows])
+        h = nxt
+    order = np.lexsort((np.arange(n),) + tuple(h[j] for j in range(num_hashes - 1, -1, -1)))
+    perm = np.empty(n, np.int64)
+    perm[order] = np.arange(n)
+    r, c = perm[rows], perm[cols]
+    return (np.maximum(r, c).astype(np.int32), np.minimum(r, c).astype(np.int32),
+            perm.astype(np.int32))
+
+
+# ---------------------------------------------------------------------------
 # reference builds (oracle/_ref)
 # ---------------------------------------------------------------------------
 
@@ -175,8 +228,24 @@ def ref_gpu():
                                   C.POINTER(C.c_ulonglong), C.POINTER(C.c_float), _f32p,
                                   C.POINTER(C.c_uint32), C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.c_void_p, C.c_int64]
+        L.ref_hashorder_gpu.restype = C.c_int
+        L.ref_hashorder_gpu.argtypes = [_i32p, _i32p, C.c_int64, C.c_int, C.c_int, C.c_int]
         _ref_gpu = L
     return _ref_gpu
+
+
+def ref_hashorder(rows, cols, n: int, num_hashes: int = 16, num_hops: int = 1):
+    """The reference's own reorder_hashorder_gpu (GPU): returns the relabelled, oriented
+    (rows, cols)."""
+    r = np.ascontiguousarray(rows, np.int32).copy()
+    c = np.ascontiguousarray(cols, np.int32).copy()
+    with _StdoutToStderr():
+        rc = ref_gpu().ref_hashorder_gpu(r if len(r) else np.zeros(1, np.int32),
+                                         c if len(c) else np.zeros(1, np.int32), len(r), int(n),
+                                         int(num_hashes), int(num_hops))
+    if rc != 0:
+        raise RuntimeError(f"ref_hashorder_gpu failed ({rc})")
+    return r, c
 
 
 class _StdoutToStderr:

@@ -7,6 +7,8 @@
 //   convert_coo_to_bcsr_16x32_gpu    btc/operations/bcsr_16x32.h:144-249
 //   count_triangles_16x128_adaptive  btc/operations/tc_16x128_adaptive.h:12-29 (threshold 2048)
 //   count_triangles_16x32_adaptive   btc/operations/tc_16x32_adaptive.h:14-31  (threshold 40000)
+// and, for the reorder step of preprocess_for_triangle_counting,
+//   reorder_hashorder_gpu            btc/operations/reorder.h:443-587
 // The only code here is the adapter from plain host arrays to the template's COO
 // member names, event timing around the convert, and copies of the result out.
 #include <cstdint>
@@ -20,6 +22,7 @@
 #include "btc/operations/bcsr_16x32.h"
 #include "btc/operations/tc_16x128_adaptive.h"
 #include "btc/operations/tc_16x32_adaptive.h"
+#include "btc/operations/reorder.h"
 
 namespace {
 struct DevCoo {
@@ -111,4 +114,23 @@ extern "C" int ref_gpu_run(const int* h_rows, const int* h_cols, int64_t nnz, in
     *out_count = count;
     if (cudaDeviceSynchronize() != cudaSuccess || cudaGetLastError() != cudaSuccess) return -2;
     return rc;
+}
+
+// The reference's GPU HashOrder on a COO of n vertices (any orientation), in place on
+// the host arrays: relabelled and oriented to (max, min) exactly as reorder_hashorder_gpu
+// leaves the device COO.  Returns 0, or -2 on a CUDA error.
+extern "C" int ref_hashorder_gpu(int* h_rows, int* h_cols, int64_t nnz, int n, int num_hashes,
+                                 int num_hops)
+{
+    DevCoo coo;
+    coo.num_rows = n;
+    coo.num_cols = n;
+    coo.num_entries = (size_t)nnz;
+    coo.row_indices.assign(h_rows, h_rows + nnz);
+    coo.column_indices.assign(h_cols, h_cols + nnz);
+    btc::reorder_hashorder_gpu(coo, num_hashes, num_hops);
+    if (cudaDeviceSynchronize() != cudaSuccess) return -2;
+    thrust::copy(coo.row_indices.begin(), coo.row_indices.end(), h_rows);
+    thrust::copy(coo.column_indices.begin(), coo.column_indices.end(), h_cols);
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
