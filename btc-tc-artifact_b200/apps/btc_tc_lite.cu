@@ -156,13 +156,30 @@ int main(int argc, char** argv)
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
 
-    // preprocess_for_triangle_counting (convert.h:600) with BTC_REORDER=0
+    // preprocess_for_triangle_counting (convert.h:600-690): orient, dedup, remap, then the
+    // reorder step BTC_REORDER selects -- 8: GPU HashOrder, 9: HashOrder when
+    // should_reorder_gpu says so (the input's base name is the hint); unset or 0: none
+    // (the reference's default is 9)
     cudaEventRecord(e0);
     int64_t nnz = (int64_t)coo.num_entries;
     int32_t rows = n;
     int st = btc_preprocess_for_triangle_counting(
         thrust::raw_pointer_cast(coo.row_indices.data()),
         thrust::raw_pointer_cast(coo.column_indices.data()), &nnz, &rows, 1);
+    const char* env_reorder = std::getenv("BTC_REORDER");
+    const int reorder_mode = env_reorder ? std::atoi(env_reorder) : 0;
+    if (st == BTC_OK && (reorder_mode == 8 || reorder_mode == 9)) {
+        int dev = 0, major = 0, minor = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+        cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
+        std::string base = path.substr(path.find_last_of('/') == std::string::npos ? 0 : path.find_last_of('/') + 1);
+        base = base.substr(0, base.find_last_of('.'));
+        if (reorder_mode == 8 || btc_should_reorder(rows, nnz, 10 * major + minor, base.c_str()))
+            st = btc_reorder_hashorder(thrust::raw_pointer_cast(coo.row_indices.data()),
+                                       thrust::raw_pointer_cast(coo.column_indices.data()), nnz,
+                                       rows, 16, 1, nullptr, nullptr);
+    }
     cudaEventRecord(e1);
     cudaEventSynchronize(e1);
     float t_pre = 0.f;

@@ -114,3 +114,24 @@ def test_hashorder_packs_low_degree_graphs_into_fewer_tiles():
     after = BitBSR(coo.row_indices, coo.column_indices, n, 32)
     assert after.count() == before.count()
     assert after.num_tiles < before.num_tiles
+
+
+@pytest.mark.parametrize("mode", ["8", "9"])
+def test_compat_cli_reorder_modes(mode, tmp_path):
+    """apps/btc_tc_lite.cu honours BTC_REORDER like the reference's preprocess (8: GPU
+    HashOrder; 9: when the automatic rule says so, which it does for this ER graph on
+    B200); the count is unchanged."""
+    import os
+    import re
+    import subprocess
+    src, dst, n = G.erdos_renyi(8192, 8, seed=2)
+    rp, col, _ = O.lower_csr(src, dst, n)
+    want = O.tc_merge(rp, col)
+    path = tmp_path / "er_8192_8.mtx"
+    G.write_mtx(str(path), src, dst, n)
+    app = os.path.join(os.path.dirname(_lib.LIB_PATH), "btc_tc_lite")
+    env = dict(os.environ, BTC_REORDER=mode)
+    out = subprocess.run([app, "-i", str(path), "-w", "1", "-r", "2"], capture_output=True,
+                         text=True, timeout=120, env=env)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert int(re.search(r"Triangles \(GPU\): (\d+)", out.stdout).group(1)) == want
