@@ -717,13 +717,32 @@ def main():
     achieved = bytes_count / tc / 1e9
     # DRAM bytes of one count launch, from the committed ncu summary of this workload
     # (dram__bytes_read.sum + dram__bytes_write.sum; a line "dram_bytes_per_launch: N")
+    # The same summary gives the warp instructions per launch (smsp__inst_executed.sum):
+    # the kernel is issue-bound, so its issue rate against the SMs' (4 schedulers per SM,
+    # one warp instruction each per cycle, at the median SM clock sampled during the
+    # timed region) says how close it runs to its real limit.
     traffic = None
+    warp_inst = None
     prof = os.path.join(ROOT, "profiles", f"count_{tile}_{args.workload}.md")
     if os.path.exists(prof):
         with open(prof) as f:
             for ln in f:
                 if ln.startswith("dram_bytes_per_launch:"):
                     traffic = int(ln.split(":", 1)[1])
+                elif "`smsp__inst_executed.sum`" in ln:
+                    warp_inst = float(ln.split("|")[2].replace(",", ""))
+    clocks = clk.summary()
+    issue = None
+    if warp_inst:
+        sms = torch.cuda.get_device_properties(local).multi_processor_count
+        mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz")
+        if mhz:
+            peak_issue = sms * 4 * mhz * 1e6
+            issue = {"warp_instructions": warp_inst, "achieved_per_s": warp_inst / tc,
+                     "peak_per_s": peak_issue, "frac": warp_inst / tc / peak_issue,
+                     "source": f"warp instructions per launch from profiles/count_{tile}_"
+                               f"{args.workload}.md; peak = {sms} SMs x 4 schedulers x "
+                               f"{mhz:g} MHz"}
 
     line = {
         "metric": METRIC,
@@ -751,10 +770,11 @@ def main():
                      "frac": achieved / hbm, "traffic": traffic,
                      "kernel": f"k_count<{tile}>", "algorithmic_bytes": bytes_count,
                      "kernel_ms": tc * 1e3, "peak_source": peak_src},
+        "issue": issue,
         "phases": {"count_ms": tc * 1e3, "build_ms": tb * 1e3,
                    "build_gbs": bytes_build / tb / 1e9,
                    "count_edges_per_s": m_lower / tc},
-        "clocks": clk.summary(),
+        "clocks": clocks,
     }
 
     if rank == 0 and world == 1:
