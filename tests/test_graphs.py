@@ -105,3 +105,25 @@ def test_batch_mix_device_on_cpu_is_seeded_and_in_range():
         if len(s):
             assert int(s.min()) >= 0 and int(s.max()) < nv[i]
             assert int(d.min()) >= 0 and int(d.max()) < nv[i]
+
+
+def test_batch_bench_groups_respect_the_launch_limit():
+    """bench.py's batch workload cuts the graphs into consecutive launches of at most
+    `limit` edges (a larger graph alone), covering every graph once, in order."""
+    import importlib.util
+    import os
+    spec = importlib.util.spec_from_file_location(
+        "bench_mod", os.path.join(os.path.dirname(os.path.dirname(__file__)), "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    rng = np.random.default_rng(4)
+    sizes = rng.integers(0, 1000, 300)
+    sizes[[7, 100]] = 5000  # larger than the limit
+    off = np.zeros(len(sizes) + 1, np.int64)
+    off[1:] = np.cumsum(sizes)
+    groups = bench.batch_groups(off, 2000)
+    assert groups[0][0] == 0 and groups[-1][1] == len(sizes)
+    for (a, b), (c, _) in zip(groups, groups[1:]):
+        assert b == c and b > a
+    for a, b in groups:
+        assert off[b] - off[a] <= 2000 or b == a + 1
