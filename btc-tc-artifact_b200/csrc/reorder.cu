@@ -197,20 +197,45 @@ extern "C" int btc_reorder_hashorder(int32_t* d_rows, int32_t* d_cols, int64_t n
     const int H = num_hashes;
     cudaStream_t s = stream;
 
-    DevBuf deg, start, cursor, nbr, hv0, hv1, k0, k1, scratch, perm, ab, meta;
-    BTC_TRY(deg.reserve(sizeof(uint32_t) * (size_t)n));
-    BTC_TRY(start.reserve(sizeof(uint32_t) * (size_t)n));
-    BTC_TRY(cursor.reserve(sizeof(uint32_t) * (size_t)n));
-    BTC_TRY(nbr.reserve(sizeof(int32_t) * (size_t)(2 * nnz > 0 ? 2 * nnz : 1)));
-    BTC_TRY(hv0.reserve(sizeof(uint32_t) * (size_t)n * H));
-    if (num_hops > 1) BTC_TRY(hv1.reserve(sizeof(uint32_t) * (size_t)n * H));
-    BTC_TRY(k0.reserve(sizeof(uint64_t) * (size_t)n));
-    BTC_TRY(k1.reserve(sizeof(uint64_t) * (size_t)n));
-    BTC_TRY(scratch.reserve(sizeof(uint32_t) * radix_scratch_words((size_t)n)));
-    if (!d_perm) BTC_TRY(perm.reserve(sizeof(int32_t) * (size_t)n));
-    BTC_TRY(ab.reserve(sizeof(uint32_t) * 2 * (size_t)H));
-    BTC_TRY(meta.reserve(sizeof(unsigned long long) * 2));
-    unsigned long long* d_meta = meta.as<unsigned long long>();  // [0] bad ids, [1] n
+    // One workspace, carved into 256-byte-aligned pieces, released on every return.
+    struct Workspace {
+        DevBuf buf;
+        ~Workspace() { buf.release(); }
+    } ws;
+    const size_t nn = (size_t)n, ne = (size_t)(2 * nnz > 0 ? 2 * nnz : 1);
+    const size_t sizes[] = {sizeof(uint32_t) * nn,                        // deg
+                            sizeof(uint32_t) * nn,                        // start
+                            sizeof(uint32_t) * nn,                        // cursor
+                            sizeof(int32_t) * ne,                         // nbr
+                            sizeof(uint32_t) * nn * H,                    // hv0
+                            num_hops > 1 ? sizeof(uint32_t) * nn * H : 0,  // hv1
+                            sizeof(uint64_t) * nn,                        // k0
+                            sizeof(uint64_t) * nn,                        // k1
+                            sizeof(uint32_t) * radix_scratch_words(nn),   // scratch
+                            d_perm ? 0 : sizeof(int32_t) * nn,            // perm
+                            sizeof(uint32_t) * 2 * (size_t)H,             // ab
+                            sizeof(unsigned long long) * 2};              // meta
+    constexpr int kParts = (int)(sizeof(sizes) / sizeof(sizes[0]));
+    size_t offs[kParts], total = 0;
+    for (int i = 0; i < kParts; ++i) {
+        offs[i] = total;
+        total += (sizes[i] + 255) & ~(size_t)255;
+    }
+    BTC_TRY(ws.buf.reserve(total));
+    char* base = ws.buf.as<char>();
+    auto part = [&](int i) { return sizes[i] ? (void*)(base + offs[i]) : nullptr; };
+    uint32_t* deg = static_cast<uint32_t*>(part(0));
+    uint32_t* start = static_cast<uint32_t*>(part(1));
+    uint32_t* cursor = static_cast<uint32_t*>(part(2));
+    int32_t* nbr = static_cast<int32_t*>(part(3));
+    uint32_t* hv0 = static_cast<uint32_t*>(part(4));
+    uint32_t* hv1 = static_cast<uint32_t*>(part(5));
+    uint64_t* k0 = static_cast<uint64_t*>(part(6));
+    uint64_t* k1 = static_cast<uint64_t*>(part(7));
+    uint32_t* scratch = static_cast<uint32_t*>(part(8));
+    int32_t* perm = static_cast<int32_t*>(part(9));
+    uint32_t* ab = static_cast<uint32_t*>(part(10));
+    unsigned long long* d_meta = static_cast<unsigned long long*>(part(11));  // [0] bad ids, [1] n
 
     std::vector<uint32_t> a(H), b(H), h_ab(2 * (size_t)H);
     hashorder_params(H, a.data(), b.data());
@@ -218,33 +243,29 @@ extern "C" int btc_reorder_hashorder(int32_t* d_rows, int32_t* d_cols, int64_t n
         h_ab[2 * (size_t)j] = a[j];
         h_ab[2 * (size_t)j + 1] = b[j];
     }
-    BTC_CUDA_TRY(cudaMemcpyAsync(ab.ptr, h_ab.data(), sizeof(uint32_t) * 2 * (size_t)H,
+    BTC_CUDA_TRY(cudaMemcpyAsync(ab, h_ab.data(), sizeof(uint32_t) * 2 * (size_t)H,
                                  cudaMemcpyHostToDevice, s));
     BTC_CUDA_TRY(cudaMemsetAsync(d_meta, 0, sizeof(unsigned long long) * 2, s));
 
     // ---- symmetric neighbour lists -------------------------------------------------
-    BTC_CUDA_TRY(cudaMemsetAsync(deg.ptr, 0, sizeof(uint32_t) * (size_t)n, s));
+    BTC_CUDA_TRY(cudaMemsetAsync(deg, 0, sizeof(uint32_t) * (size_t)n, s));
     const int eg = grid_for(nnz > 0 ? nnz : 1, 256), vg = grid_for(n, 256);
     if (nnz > 0)
-        ro::k_degree2<<<eg, 256, 0, s>>>(d_rows, d_cols, nnz, n, deg.as<uint32_t>(), d_meta);
-    BTC_CUDA_TRY(cudaMemcpyAsync(start.ptr, deg.ptr, sizeof(uint32_t) * (size_t)n,
+        ro::k_degree2<<<eg, 256, 0, s>>>(d_rows, d_cols, nnz, n, deg, d_meta);
+    BTC_CUDA_TRY(cudaMemcpyAsync(start, deg, sizeof(uint32_t) * (size_t)n,
                                  cudaMemcpyDeviceToDevice, s));
-    BTC_TRY(launch_tile_scan(start.as<uint32_t>(), (uint32_t)n, d_meta + 1, s));
-    BTC_CUDA_TRY(cudaMemcpyAsync(cursor.ptr, start.ptr, sizeof(uint32_t) * (size_t)n,
+    BTC_TRY(launch_tile_scan(start, (uint32_t)n, d_meta + 1, s));
+    BTC_CUDA_TRY(cudaMemcpyAsync(cursor, start, sizeof(uint32_t) * (size_t)n,
                                  cudaMemcpyDeviceToDevice, s));
     if (nnz > 0)
-        ro::k_scatter2<<<eg, 256, 0, s>>>(d_rows, d_cols, nnz, n, cursor.as<uint32_t>(),
-                                          nbr.as<int32_t>());
+        ro::k_scatter2<<<eg, 256, 0, s>>>(d_rows, d_cols, nnz, n, cursor, nbr);
 
     // ---- signatures ------------------------------------------------------------------
-    ro::k_minhash_first<<<vg, 256, 0, s>>>(start.as<uint32_t>(), deg.as<uint32_t>(),
-                                           nbr.as<int32_t>(), n, H, num_hops,
-                                           ab.as<uint32_t>(), hv0.as<uint32_t>());
-    uint32_t* hin = hv0.as<uint32_t>();
-    uint32_t* hout = hv1.as<uint32_t>();
+    ro::k_minhash_first<<<vg, 256, 0, s>>>(start, deg, nbr, n, H, num_hops, ab, hv0);
+    uint32_t* hin = hv0;
+    uint32_t* hout = hv1;
     for (int hop = 1; hop < num_hops; ++hop) {
-        ro::k_minhash_hop<<<vg, 256, 0, s>>>(start.as<uint32_t>(), deg.as<uint32_t>(),
-                                             nbr.as<int32_t>(), n, H, hin, hout);
+        ro::k_minhash_hop<<<vg, 256, 0, s>>>(start, deg, nbr, n, H, hin, hout);
         std::swap(hin, hout);
     }
     BTC_CUDA_TRY(cudaGetLastError());
@@ -252,13 +273,13 @@ extern "C" int btc_reorder_hashorder(int32_t* d_rows, int32_t* d_cols, int64_t n
     // ---- lexicographic order: least significant hash first, stable ------------------
     BTC_TRY(launch_set_u64(d_meta + 1, (unsigned long long)n, s));
     const uint64_t* prev = nullptr;
-    uint64_t* keys = k0.as<uint64_t>();
-    uint64_t* alt = k1.as<uint64_t>();
+    uint64_t* keys = k0;
+    uint64_t* alt = k1;
     for (int j = H - 1; j >= 0; --j) {
         ro::k_sig_keys<<<vg, 256, 0, s>>>(prev, n, hin + (size_t)j * n, keys);
         int st = BTC_OK;
         uint64_t* sorted = radix_sort_u64(keys, alt, (size_t)n, d_meta + 1, 32, 64,
-                                          scratch.as<uint32_t>(), s, &st);
+                                          scratch, s, &st);
         BTC_TRY(st);
         // the next pass reads `sorted` and writes the other buffer
         uint64_t* other = sorted == keys ? alt : keys;
@@ -268,7 +289,7 @@ extern "C" int btc_reorder_hashorder(int32_t* d_rows, int32_t* d_cols, int64_t n
     }
 
     // ---- relabel -----------------------------------------------------------------------
-    int32_t* p = d_perm ? d_perm : perm.as<int32_t>();
+    int32_t* p = d_perm ? d_perm : perm;
     BTC_TRY(launch_rank_scatter(prev, n, p, s));
     unsigned long long h_bad = 0;
     BTC_CUDA_TRY(cudaMemcpyAsync(&h_bad, d_meta, sizeof(h_bad), cudaMemcpyDeviceToHost, s));
