@@ -175,10 +175,16 @@ int main(int argc, char** argv)
         cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
         std::string base = path.substr(path.find_last_of('/') == std::string::npos ? 0 : path.find_last_of('/') + 1);
         base = base.substr(0, base.find_last_of('.'));
+        // the signature size and hop count come from BTC_HASHORDER_HASHES / _HOPS, 16 and
+        // 1 when unset, as convert.h:668-683 reads them
+        const char* env_hashes = std::getenv("BTC_HASHORDER_HASHES");
+        const char* env_hops = std::getenv("BTC_HASHORDER_HOPS");
+        const int ho_hashes = env_hashes ? std::atoi(env_hashes) : 16;
+        const int ho_hops = env_hops ? std::atoi(env_hops) : 1;
         if (reorder_mode == 8 || btc_should_reorder(rows, nnz, 10 * major + minor, base.c_str()))
             st = btc_reorder_hashorder(thrust::raw_pointer_cast(coo.row_indices.data()),
                                        thrust::raw_pointer_cast(coo.column_indices.data()), nnz,
-                                       rows, 16, 1, nullptr, nullptr);
+                                       rows, ho_hashes, ho_hops, nullptr, nullptr);
     }
     cudaEventRecord(e1);
     cudaEventSynchronize(e1);

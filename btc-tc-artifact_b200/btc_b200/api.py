@@ -106,7 +106,29 @@ def preprocess_for_triangle_counting(coo: CooMatrix, force_cpu: bool = False,
     coo.num_rows = coo.num_cols = int(rows.value)
     hint = os.path.splitext(os.path.basename(input_file))[0] if input_file else ""
     if reorder == 8 or (reorder == 9 and should_reorder_gpu(coo, hint)):
-        reorder_hashorder_gpu(coo)
+        hashes, hops = hashorder_env()
+        reorder_hashorder_gpu(coo, hashes, hops)
+
+
+def hashorder_env() -> tuple[int, int]:
+    """(num_hashes, num_hops) for the HashOrder step of preprocess_for_triangle_counting:
+    BTC_HASHORDER_HASHES and BTC_HASHORDER_HOPS, 16 and 1 when unset (convert.h:668-683,
+    which parses them with atoi)."""
+    def atoi(name: str, default: int) -> int:
+        v = os.environ.get(name)
+        if v is None:
+            return default
+        digits = ""
+        for ch in v.strip():
+            if ch.isdigit() or (not digits and ch in "+-"):
+                digits += ch
+            else:
+                break
+        try:
+            return int(digits)
+        except ValueError:
+            return 0
+    return atoi("BTC_HASHORDER_HASHES", 16), atoi("BTC_HASHORDER_HOPS", 1)
 
 
 def reorder_hashorder_gpu(coo: CooMatrix, num_hashes: int = 16, num_hops: int = 1):

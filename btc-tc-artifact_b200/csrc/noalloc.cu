@@ -10,6 +10,8 @@
 // keeps that scratch in g_noalloc_scratch, a fixed array that is part of the library's
 // device image; the caller passes only the Bit-BSR it already holds and a device word
 // for the count.
+#include <cuda.h>
+
 #include <cstdio>
 #include <mutex>
 
@@ -26,27 +28,65 @@ constexpr int kNoAllocMaxCtas = 2048;
 static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocMaxCtas + 2];
 
 constexpr int kMaxDevices = 64;
+struct ScratchSetup {
+    unsigned long long ctx_id = 0;      // context the address belongs to (0: none yet)
+    unsigned long long* addr = nullptr;
+};
 std::mutex g_setup_mu;
-unsigned long long* g_scratch_addr[kMaxDevices] = {};
+ScratchSetup g_setup[kMaxDevices];
+
+// Unique id of the current context (driver API through the runtime's entry-point table,
+// so the library needs no link against libcuda); 0 when there is none yet.
+unsigned long long current_context_id()
+{
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(f);
+        cudaGetLastError();
+    });
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+    if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
 
 // Device address of g_noalloc_scratch on the current device.  In host code the array's
-// name is only a host-side handle, so the address comes from cudaGetSymbolAddress, once
-// per device, with that device current.
+// name is only a host-side handle, so the address comes from cudaGetSymbolAddress, with
+// the device current, once per device and context: a device reset (cudaDeviceReset)
+// gives the device a new context and the next call looks the address up again.
 int scratch_for_current_device(unsigned long long** out)
 {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return BTC_E_CUDA;
     std::lock_guard<std::mutex> lock(g_setup_mu);
-    if (!g_scratch_addr[dev]) {
+    ScratchSetup& su = g_setup[dev];
+    const unsigned long long id = current_context_id();
+    if (!su.addr || id == 0 || id != su.ctx_id) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p) {
             note_cuda_error(e, "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
             return BTC_E_CUDA;
         }
-        g_scratch_addr[dev] = static_cast<unsigned long long*>(p);
+        su.addr = static_cast<unsigned long long*>(p);
+        // the lookup made the context current if there was none; a context whose id
+        // cannot be read is looked up again on every call
+        su.ctx_id = id ? id : current_context_id();
     }
-    *out = g_scratch_addr[dev];
+    *out = su.addr;
     return BTC_OK;
 }
 

@@ -257,6 +257,13 @@ extern "C" int btc_reorder_hashorder(int32_t* d_rows, int32_t* d_cols, int64_t n
     BTC_TRY(launch_tile_scan(start, (uint32_t)n, d_meta + 1, s));
     BTC_CUDA_TRY(cudaMemcpyAsync(cursor, start, sizeof(uint32_t) * (size_t)n,
                                  cudaMemcpyDeviceToDevice, s));
+    // An out-of-range id fails the call before anything reaches the caller's arrays
+    // (neither d_perm nor the COO is written).
+    unsigned long long h_bad = 0;
+    BTC_CUDA_TRY(cudaGetLastError());
+    BTC_CUDA_TRY(cudaMemcpyAsync(&h_bad, d_meta, sizeof(h_bad), cudaMemcpyDeviceToHost, s));
+    BTC_CUDA_TRY(cudaStreamSynchronize(s));
+    if (h_bad) return BTC_E_RANGE;
     if (nnz > 0)
         ro::k_scatter2<<<eg, 256, 0, s>>>(d_rows, d_cols, nnz, n, cursor, nbr);
 
@@ -291,10 +298,6 @@ extern "C" int btc_reorder_hashorder(int32_t* d_rows, int32_t* d_cols, int64_t n
     // ---- relabel -----------------------------------------------------------------------
     int32_t* p = d_perm ? d_perm : perm;
     BTC_TRY(launch_rank_scatter(prev, n, p, s));
-    unsigned long long h_bad = 0;
-    BTC_CUDA_TRY(cudaMemcpyAsync(&h_bad, d_meta, sizeof(h_bad), cudaMemcpyDeviceToHost, s));
-    BTC_CUDA_TRY(cudaStreamSynchronize(s));
-    if (h_bad) return BTC_E_RANGE;  // nothing relabelled
     if (nnz > 0) ro::k_relabel<<<eg, 256, 0, s>>>(d_rows, d_cols, nnz, p);
     BTC_CUDA_TRY(cudaGetLastError());
     BTC_CUDA_TRY(cudaStreamSynchronize(s));

@@ -126,8 +126,8 @@ BTC_API int btc_preprocess_for_triangle_counting(int32_t* d_rows, int32_t* d_col
  * (2^32 - 5) with the reference's parameters (btc_hashorder_params); order: lexicographic
  * by signature, ties by id.  The reference's defaults are num_hashes 16, num_hops 1.
  * d_perm (nullable, num_rows int32) receives new id = d_perm[old id].  Ids outside
- * [0, num_rows) give BTC_E_RANGE and leave the COO unchanged.  Allocates its workspace;
- * blocking. */
+ * [0, num_rows) give BTC_E_RANGE and leave both the COO and d_perm unwritten.  Allocates
+ * its workspace; blocking. */
 BTC_API int btc_reorder_hashorder(int32_t* d_rows, int32_t* d_cols, int64_t nnz, int32_t num_rows,
                                   int num_hashes, int num_hops, int32_t* d_perm,
                                   btc_stream_t stream);
@@ -210,9 +210,13 @@ BTC_API int btc_count(btc_bitbsr* g, int tau, btc_stream_t stream, unsigned long
  * whose count grid needs more than 2048 CTAs is rejected with BTC_E_INVAL and a message
  * on stderr (a B200 needs 592).  The first call on each device looks up the array's
  * device address (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture.  All calls share the one array: calls whose kernels overlap
- * on the GPU (different streams, or several host threads) race and give wrong counts, so
- * order them.  Stream-ordered; does not wait for the result.  tau as in btc_count. */
+ * before any stream capture.  A device reset (cudaDeviceReset) gives the device a new
+ * context, and the next call repeats that lookup, so it too should come before any
+ * capture.  All calls share the one array: calls whose kernels overlap on the GPU
+ * (different streams, or several host threads) race and give wrong counts, so order
+ * them.  It always runs the count's light variant (it has no per-tile row masks), so on
+ * power-law graphs, where btc_count picks the heavy variant, it is exact but slower.
+ * Stream-ordered; does not wait for the result.  tau as in btc_count. */
 BTC_API int btc_count_bcsr_noalloc(const btc_bcsr_device* bcsr, int tile_cols, int tau,
                                    btc_stream_t stream, unsigned long long* d_out);
 

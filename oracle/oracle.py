@@ -36,9 +36,10 @@ _ref_gpu = None
 
 
 def build(ref: bool = True) -> None:
-    """Compile liboracle.so and, when the reference tree is present, oracle/_ref."""
+    """Compile liboracle.so and, when a reference checkout is present (oracle/ref/Makefile
+    finds it, or BTC_REF_DIR names it), oracle/_ref."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    if ref and os.path.isdir("/root/reference"):
+    if ref:
         subprocess.run(["make", "-s", "-C", os.path.join(HERE, "ref")], check=True)
 
 
@@ -94,6 +95,14 @@ def tc_merge(rowptr, col, threads: int = 0) -> int:
     if len(col) == 0:
         col = np.zeros(1, np.int32)
     return int(lib().orc_tc_merge(rowptr, col, len(rowptr) - 1, threads))
+
+
+def bitbsr_num_tiles(rowptr, col, n: int, tile_cols: int) -> int:
+    """Number of tiles of the Bit-BSR of a lower CSR (no arrays built)."""
+    rowptr, col = _i32(rowptr), _i32(col)
+    if len(col) == 0:
+        col = np.zeros(1, np.int32)
+    return int(lib().orc_bitbsr_num_tiles(rowptr, col, n, tile_cols))
 
 
 def bitbsr_build(rowptr, col, n: int, tile_cols: int):
