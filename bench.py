@@ -1,14 +1,17 @@
 """Benchmark: exact triangle counting (Bit-BSR build + hybrid count) on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
-                    [--workload stencil27_64|er_16384|rmat22_deg] [--tile 0|32|128]
+                    [--workload rmat22_deg|stencil27_64|er_16384|batch|serve|dense]
+                    [--tile 0|32|128]
 
 A step is one pass of the hot path over one graph: build the Bit-BSR from the raw
 undirected edge list (orient, dedup, tile) and count its triangles.  The default
-workload is the 27-point stencil on a 64^3 grid (262,144 vertices, 3,298,428 edges,
-natural lexicographic order, 16x128 tiles; 11,049,696 triangles).  The metric is
-unique undirected edges per second (whole job; N ranks each count a replica of the
-graph: weak scaling, no data-path collective).
+workload is the largest single-GPU graph: R-MAT scale 22, edge factor 16, seed 7
+(67,108,864 raw draws generated on the GPU, ~64M unique edges), ordered by
+descending degree on the GPU, 16x128 tiles; every count must equal the golden count
+the reference's CPU path gave (tests/golden).  The metric is unique undirected edges
+per second (whole job; N ranks each count a replica of the graph: weak scaling, no
+data-path collective).
 
   value      device-resident edge list in HBM, L2 flushed (512 MB write) before
              every timed step, CUDA events around each step, max over ranks
@@ -19,6 +22,9 @@ graph: weak scaling, no data-path collective).
   cpu_baseline   the reference's own cpu_tc_intersection_lower_triangular
              (oracle/_ref/libref_cpu.so, all host threads) on the same L
   --impl reference   times that same reference CPU path as the reference arm
+
+A count that differs from the golden count, or a baseline whose count differs from
+the engine's, ends the run with a non-zero exit status.
 
 Only rank 0 prints, and only one JSON line, to stdout.
 """
@@ -57,21 +63,54 @@ def peaks():
     return 6650.0, "fallback 6.65 TB/s"
 
 
-def workload(name: str):
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def golden_count(fixture: str) -> int:
+    """Triangle count of a fixture graph, computed by the reference's own CPU path when the
+    fixture files were made (tests/golden/make_golden.py)."""
+    for fn in ("golden.json", "golden_large.json"):
+        p = os.path.join(GOLDEN, fn)
+        if os.path.exists(p):
+            with open(p) as f:
+                fx = json.load(f)["fixtures"]
+            if fixture in fx:
+                return int(fx[fixture]["count"])
+    raise SystemExit(f"no golden count for {fixture}")
+
+
+def workload(name: str, device="cuda"):
+    """(src, dst, n, meta): int32 torch tensors on `device` holding the raw input pairs."""
+    import torch
     from btc_b200 import graphs as G
-    if name == "stencil27_64":
-        src, dst, n = G.stencil27(64)
-        return src, dst, n, dict(workload="27-point stencil 64^3, natural order", tile_cols=128,
-                                 expected=11049696)
-    if name == "er_16384":
-        src, dst, n = G.erdos_renyi(16384, 16, seed=1)
-        return src, dst, n, dict(workload="Erdos-Renyi n=16384 mean degree 16 seed 1",
-                                 tile_cols=0, expected=None)
     if name == "rmat22_deg":
-        src, dst, n = G.rmat(22, 16, seed=7)
-        return src, dst, n, dict(workload="R-MAT scale 22 ef 16 seed 7, GPU descending-degree order",
-                                 tile_cols=128, expected=None, orient_degree=True)
-    raise SystemExit(f"unknown workload {name}")
+        src, dst, n = G.rmat_raw_torch(22, 16, seed=7, device=device)
+        return src, dst, n, dict(
+            workload="R-MAT scale 22 ef 16 (a,b,c)=(.57,.19,.19) seed 7, raw draws "
+                     "(self-loops, duplicates) deduplicated and ordered by descending degree "
+                     "on the GPU", tile_cols=128, expected=golden_count("rmat_raw_22_16_s7"),
+            orient_degree=True)
+    if name == "stencil27_64":
+        s_, d_, n = G.stencil27(64)
+        meta = dict(workload="27-point stencil 64^3, natural order", tile_cols=128,
+                    expected=golden_count("stencil27_64"))
+    elif name == "er_16384":
+        s_, d_, n = G.erdos_renyi(16384, 16, seed=1)
+        meta = dict(workload="Erdos-Renyi n=16384 mean degree 16 seed 1", tile_cols=0,
+                    expected=golden_count("er_16384_16_s1"))
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    return (torch.from_numpy(s_).to(device), torch.from_numpy(d_).to(device), n, meta)
+
+
+def count_profile(workload_name: str, tile: int):
+    """ncu figures of one count launch on this workload (profiles/count_kernel.json): DRAM
+    bytes (read + write) and warp instructions per launch, with how they were taken."""
+    p = os.path.join(ROOT, "profiles", "count_kernel.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        return json.load(f).get(f"{workload_name}/{tile}")
 
 
 class ClockSampler:
@@ -175,35 +214,51 @@ def cpu_reference(rowptr, col, m_lower, budget_s=10.0):
 
 
 def run_reference(args, rank, world):
-    """Reference arm: the reference's CPU path on the host cores (rank 0 only)."""
+    """Reference arm: the reference's own CPU count (cpu_tc_intersection_lower_triangular,
+    oracle/_ref/libref_cpu.so, all host threads) on the same L as the engine's arm (same
+    graph, same vertex order), rank 0 only.  A step is one count of the whole graph; when
+    one count takes more than a second (R-MAT scale 22: several seconds on 16 cores) a
+    single untimed warm-up count replaces the W warm-up steps, so that the run stays
+    within a few minutes."""
     if rank != 0:
         return
     from oracle import oracle as O
-    src, dst, n, meta = workload(args.workload)
     if not O.ref_cpu_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_cpu.so not built"}))
         return
-    rp, col, _ = O.lower_csr(src, dst, n)
+    src, dst, n, meta = workload(args.workload, device="cpu")
+    odeg = bool(meta.get("orient_degree", False))
+    rp, col, _ = O.lower_csr(src.numpy(), dst.numpy(), n, "degree" if odeg else "natural")
     m_lower = len(col)
     threads = os.cpu_count() or 1
-    for _ in range(args.warmup):
+    t0 = time.perf_counter()
+    cnt = O.ref_cpu_count(rp, col, threads)
+    first_s = time.perf_counter() - t0
+    if cnt != meta["expected"]:
+        raise SystemExit(f"reference CPU count {cnt} != golden {meta['expected']}")
+    warm = args.warmup if first_s <= 1.0 else 0
+    for _ in range(max(warm - 1, 0)):
         O.ref_cpu_count(rp, col, threads)
     times = []
-    cnt = None
     for _ in range(args.steps):
         t0 = time.perf_counter()
         cnt = O.ref_cpu_count(rp, col, threads)
         times.append(time.perf_counter() - t0)
+        if cnt != meta["expected"]:
+            raise SystemExit(f"reference CPU count {cnt} != golden {meta['expected']}")
     total = sum(times)
     value = m_lower * args.steps / total
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "steps": args.steps, "warmup": args.warmup if first_s <= 1.0 else 1,
+        "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic", "config": {"workload": meta["workload"], "edges": m_lower,
-                                        "count": cnt, "parallelism": f"openmp{threads}"},
+                                        "count": cnt, "parallelism": f"openmp{threads}",
+                                        "orientation": "descending degree" if odeg else "natural id"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
-                         "sample": f"full graph, {args.steps} counts of the lower CSR"},
+                         "sample": f"full graph ({m_lower} edges), {args.steps} counts of the "
+                                   f"lower CSR"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -539,7 +594,7 @@ def main():
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--workload", default="stencil27_64")
+    ap.add_argument("--workload", default="rmat22_deg")
     ap.add_argument("--tile", type=int, default=None)
     ap.add_argument("--no-ref-gpu", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=8.0)
@@ -584,25 +639,22 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     from btc_b200 import BitBSR
-    src, dst, n, meta = workload(args.workload)
+    d_src, d_dst, n, meta = workload(args.workload, device=f"cuda:{local}")
     tile = args.tile if args.tile is not None else meta["tile_cols"]
     odeg = bool(meta.get("orient_degree", False))
-    m_in = len(src)
-    h_src = torch.from_numpy(src).pin_memory()
-    h_dst = torch.from_numpy(dst).pin_memory()
-    d_src = h_src.cuda()
-    d_dst = h_dst.cuda()
+    m_in = int(d_src.numel())
+    h_src = d_src.cpu().pin_memory()
+    h_dst = d_dst.cpu().pin_memory()
     np_src, np_dst = h_src.numpy(), h_dst.numpy()
     stream = torch.cuda.current_stream()
 
     g = BitBSR(d_src, d_dst, n, tile, orient_degree=odeg, stream=stream)
     tile = g.tile_cols
     m_lower = g.num_edges
-    expected = meta["expected"]
+    expected = int(meta["expected"])
     first = g.count(stream=stream)
-    if expected is not None and first != expected:
-        raise SystemExit(f"count {first} != expected {expected}")
-    expected = first
+    if first != expected:
+        raise SystemExit(f"count {first} != golden {expected} (reference CPU count)")
     info = g.info()
     B = int(info.bcsr.num_blocks)
     R = int(info.bcsr.n_row_blocks)
@@ -648,7 +700,7 @@ def main():
     step_ms = [e0.elapsed_time(e1) for e0, e1 in ev]
     total_ms = sum(step_ms)
     if int(d_out.item()) != expected:
-        raise SystemExit("count mismatch in timed loop")
+        raise SystemExit(f"count {int(d_out.item())} != golden {expected} in the timed loop")
     if dist:
         t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -662,7 +714,8 @@ def main():
     for _ in range(reps):
         flush.zero_()
         cnt, ms = g.count(stream=stream, timing=True)
-        assert cnt == expected
+        if cnt != expected:
+            raise SystemExit(f"count {cnt} != golden {expected}")
         t_count.append(ms)
         flush.zero_()
         b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -672,7 +725,7 @@ def main():
         torch.cuda.synchronize()
         t_build.append(b0.elapsed_time(b1))
     warm = []
-    for _ in range(20):
+    for _ in range(min(reps, 20)):
         cnt, ms = g.count(stream=stream, timing=True)
         warm.append(ms)
     tc_warm = statistics.median(warm)
@@ -683,7 +736,8 @@ def main():
     e2e_steps = min(args.steps, 100)
     for _ in range(3):
         g.rebuild(np_src, np_dst, n, tile, orient_degree=odeg, stream=stream)
-        assert g.count(stream=stream) == expected
+        if g.count(stream=stream) != expected:
+            raise SystemExit("e2e warm-up count differs from the golden count")
     torch.cuda.synchronize()
     # A step: the edge list copied from pinned host memory, the build, the count into a
     # device word and that word copied back into pinned host memory, all on `stream`; the
@@ -702,7 +756,8 @@ def main():
         e1.record(stream)
         e1.synchronize()
         cnt = int(h_out[0])
-        assert cnt == expected
+        if cnt != expected:
+            raise SystemExit(f"e2e count {cnt} != golden {expected}")
         e2e_ms.append(e0.elapsed_time(e1))
     e2e_total = sum(e2e_ms)
     if dist:
@@ -715,22 +770,15 @@ def main():
     bytes_count = 4 * (R + 1) + 8 * B + tw_bytes * B + 8
     bytes_build = 8 * m_in + 4 * (R + 1) + 8 * B + tw_bytes * B
     achieved = bytes_count / tc / 1e9
-    # DRAM bytes of one count launch, from the committed ncu summary of this workload
-    # (dram__bytes_read.sum + dram__bytes_write.sum; a line "dram_bytes_per_launch: N")
-    # The same summary gives the warp instructions per launch (smsp__inst_executed.sum):
-    # the kernel is issue-bound, so its issue rate against the SMs' (4 schedulers per SM,
-    # one warp instruction each per cycle, at the median SM clock sampled during the
-    # timed region) says how close it runs to its real limit.
-    traffic = None
-    warp_inst = None
-    prof = os.path.join(ROOT, "profiles", f"count_{tile}_{args.workload}.md")
-    if os.path.exists(prof):
-        with open(prof) as f:
-            for ln in f:
-                if ln.startswith("dram_bytes_per_launch:"):
-                    traffic = int(ln.split(":", 1)[1])
-                elif "`smsp__inst_executed.sum`" in ln:
-                    warp_inst = float(ln.split("|")[2].replace(",", ""))
+    # DRAM bytes and warp instructions of one count launch on this workload, from the
+    # committed ncu data (profiles/count_kernel.json; per launch, scaled from a smaller
+    # capture of the same graph family when the full size is too large to capture).  The
+    # kernel is issue-bound, so its warp-instruction rate against the SMs' (4 schedulers
+    # per SM, one warp instruction each per cycle, at the median SM clock sampled during
+    # the timed region) says how close it runs to its real limit.
+    prof = count_profile(args.workload, tile)
+    traffic = int(prof["dram_bytes_per_launch"]) if prof else None
+    warp_inst = float(prof["warp_instructions_per_launch"]) if prof else None
     clocks = clk.summary()
     issue = None
     if warp_inst:
@@ -740,9 +788,8 @@ def main():
             peak_issue = sms * 4 * mhz * 1e6
             issue = {"warp_instructions": warp_inst, "achieved_per_s": warp_inst / tc,
                      "peak_per_s": peak_issue, "frac": warp_inst / tc / peak_issue,
-                     "source": f"warp instructions per launch from profiles/count_{tile}_"
-                               f"{args.workload}.md; peak = {sms} SMs x 4 schedulers x "
-                               f"{mhz:g} MHz"}
+                     "source": f"warp instructions per launch: {prof['source']}; peak = "
+                               f"{sms} SMs x 4 schedulers x {mhz:g} MHz"}
 
     line = {
         "metric": METRIC,
@@ -759,6 +806,7 @@ def main():
         "data": "synthetic",
         "config": {"workload": meta["workload"], "vertices": n, "edges": m_lower,
                    "input_pairs": m_in, "tile": f"16x{tile}", "tiles": B, "triangles": expected,
+                   "triangles_source": "golden count from the reference's CPU path",
                    "orientation": "descending degree" if odeg else "natural id",
                    "parallelism": (f"tile-sharded x{world}, int64 all-reduce" if args.shard
                                    else f"replica x{world}" if world > 1 else "single GPU"),
@@ -768,6 +816,7 @@ def main():
         "gpu_launches": launches_per_step(n, tile, odeg, m_in) * args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": traffic,
+                     "traffic_source": prof["source"] if prof else None,
                      "kernel": f"k_count<{tile}>", "algorithmic_bytes": bytes_count,
                      "kernel_ms": tc * 1e3, "peak_source": peak_src},
         "issue": issue,
@@ -778,30 +827,36 @@ def main():
     }
 
     if rank == 0 and world == 1:
+        # Baselines on the same L.  A baseline that is not built is skipped; a baseline
+        # whose count differs from the engine's ends the run with an error.
         from oracle import oracle as O
-        try:
-            rp, col, _ = O.lower_csr(src, dst, n, "degree" if odeg else "natural")
-            if O.ref_cpu_available():
-                cnt, t, threads, reps_cpu = cpu_reference(rp, col, m_lower, args.cpu_budget)
-                assert cnt == expected, (cnt, expected)
-                line["cpu_baseline"] = {"value": m_lower / t, "unit": UNIT, "cores": threads,
-                                        "kind": "reference",
-                                        "sample": f"full graph, median of {reps_cpu} counts"}
-            if O.ref_gpu_available() and not args.no_ref_gpu:
-                rr, cc = rp_to_coo(rp, col)
-                big = B > 2_000_000
-                ref = O.ref_gpu_run(rr, cc, n, tile, warmup=1 if big else 3, repeat=3 if big else 20)
-                assert ref["count"] == expected, (ref["count"], expected)
-                kms = statistics.median(ref["kernel_ms"])
-                line["reference_gpu"] = {
-                    "what": "reference convert + adaptive count compiled for sm_100a, same box",
-                    "convert_ms": ref["convert_ms"], "kernel_ms": kms,
-                    "engine_build_ms": tb * 1e3, "engine_count_ms_l2_flushed": tc * 1e3,
-                    "engine_count_ms_l2_warm": tc_warm,
-                    "count_speedup_same_l2_state": kms / tc_warm,
-                    "note": "reference kernel timed by its own events, L2 warm"}
-        except Exception as e:  # baselines are reported, never required
-            log("baseline leg failed:", repr(e))
+        rp, col, _ = O.lower_csr(np_src, np_dst, n, "degree" if odeg else "natural")
+        if O.ref_cpu_available():
+            cnt, t, threads, reps_cpu = cpu_reference(rp, col, m_lower, args.cpu_budget)
+            if cnt != expected:
+                raise SystemExit(f"reference CPU count {cnt} != engine count {expected}")
+            line["cpu_baseline"] = {"value": m_lower / t, "unit": UNIT, "cores": threads,
+                                    "kind": "reference",
+                                    "sample": f"full graph ({m_lower} edges), median of "
+                                              f"{reps_cpu} counts"}
+        else:
+            log("cpu baseline unavailable: oracle/_ref/libref_cpu.so not built")
+        if O.ref_gpu_available() and not args.no_ref_gpu:
+            rr, cc = rp_to_coo(rp, col)
+            big = B > 2_000_000
+            ref = O.ref_gpu_run(rr, cc, n, tile, warmup=1 if big else 3, repeat=3 if big else 20)
+            if ref["count"] != expected:
+                raise SystemExit(f"reference GPU count {ref['count']} != engine count {expected}")
+            kms = statistics.median(ref["kernel_ms"])
+            line["reference_gpu"] = {
+                "what": "reference convert + adaptive count compiled for sm_100a, same box",
+                "convert_ms": ref["convert_ms"], "kernel_ms": kms,
+                "engine_build_ms": tb * 1e3, "engine_count_ms_l2_flushed": tc * 1e3,
+                "engine_count_ms_l2_warm": tc_warm,
+                "count_speedup_same_l2_state": kms / tc_warm,
+                "note": "reference kernel timed by its own events, L2 warm"}
+        else:
+            log("reference GPU leg unavailable or disabled")
     if rank == 0:
         print(json.dumps(line), flush=True)
     g.free()

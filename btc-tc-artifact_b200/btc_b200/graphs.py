@@ -10,6 +10,8 @@ Workloads (sizes as used by bench.py):
   * ``stencil27(64)``                      27-point 3-D stencil, 262,144 vertices,
                                            3,298,428 edges, 11,049,696 triangles
   * ``rmat(22, 16, seed=7)``               R-MAT (.57,.19,.19,.05), ~64M edges
+  * ``rmat_raw_torch(22, 16, seed=7)``     the same shape, counter-based draws generated
+                                           on the GPU (``rmat_raw_np``: the CPU twin)
   * ``sbm(n, 8, p_in, 0.001, seed)``       8-community stochastic block model
   * ``stencil7(k)``                        7-point stencil (bipartite: 0 triangles)
   * ``complete(n)``                        K_n (C(n,3) triangles)
@@ -118,6 +120,103 @@ def rmat(scale: int, edge_factor: int, a=0.57, b=0.19, c=0.19, seed: int = 7,
     src, dst, n = _pairs_to_edges(u, v, n, rng)
     if degree_order:
         src, dst = relabel_by_degree(src, dst, n)
+    return src, dst, n
+
+
+# Counter-based R-MAT: the quadrant of draw i at level l comes from a 64-bit hash of
+# (seed, i, l) (the splitmix64 finaliser), compared as an integer with thresholds
+# round(p * 2^32).  The numpy and torch versions below give identical draws on any
+# device, so a graph generated on the GPU in milliseconds has the count computed once on
+# the CPU from the numpy version.
+_SM_GAMMA = 0x9E3779B97F4A7C15
+_SM_M1 = 0xBF58476D1CE4E5B9
+_SM_M2 = 0x94D049BB133111EB
+_M64 = (1 << 64) - 1
+
+
+def _rmat_thresholds(a, b, c):
+    return (int(round(a * 2 ** 32)), int(round((a + b) * 2 ** 32)),
+            int(round((a + b + c) * 2 ** 32)))
+
+
+def _rmat_key_base(seed: int) -> int:
+    return (int(seed) * _SM_GAMMA) & _M64
+
+
+def rmat_raw_np(scale: int, edge_factor: int, seed: int = 7, a=0.57, b=0.19, c=0.19):
+    """Raw counter-based R-MAT draws (self-loops and duplicates kept; the engine's
+    builder and the oracle's lower_csr remove them) as int32 numpy arrays, plus n.
+    Draw i's bit at level l (first level = most significant): the top 32 bits x of
+    splitmix64(seed * gamma + 64 * i + l) pick the quadrant -- row bit x >= (a+b),
+    column bit a <= x < a+b or x >= a+b+c, thresholds scaled by 2^32."""
+    ta, tab, tabc = _rmat_thresholds(a, b, c)
+    n = 1 << scale
+    m = edge_factor << scale
+    base = np.uint64(_rmat_key_base(seed))
+    src = np.empty(m, np.int32)
+    dst = np.empty(m, np.int32)
+    chunk = 1 << 22
+    with np.errstate(over="ignore"):
+        for s0 in range(0, m, chunk):
+            e0 = min(m, s0 + chunk)
+            key0 = np.arange(s0, e0, dtype=np.uint64) * np.uint64(64) + base
+            u = np.zeros(e0 - s0, np.uint32)
+            v = np.zeros(e0 - s0, np.uint32)
+            for lev in range(scale):
+                z = key0 + np.uint64(lev) + np.uint64(_SM_GAMMA)
+                z = (z ^ (z >> np.uint64(30))) * np.uint64(_SM_M1)
+                z = (z ^ (z >> np.uint64(27))) * np.uint64(_SM_M2)
+                z = z ^ (z >> np.uint64(31))
+                x = z >> np.uint64(32)
+                row = x >= np.uint64(tab)
+                col = ((x >= np.uint64(ta)) & (x < np.uint64(tab))) | (x >= np.uint64(tabc))
+                u = (u << np.uint32(1)) | row.astype(np.uint32)
+                v = (v << np.uint32(1)) | col.astype(np.uint32)
+            src[s0:e0] = u.astype(np.int32)
+            dst[s0:e0] = v.astype(np.int32)
+    return src, dst, n
+
+
+def _as_signed64(x: int) -> int:
+    x &= _M64
+    return x - (1 << 64) if x >> 63 else x
+
+
+def rmat_raw_torch(scale: int, edge_factor: int, seed: int = 7, a=0.57, b=0.19, c=0.19,
+                   device="cuda"):
+    """rmat_raw_np's draws generated by torch on `device` (int64 arithmetic wraps
+    modulo 2^64; right shifts are made logical by masking).  Returns int32 tensors
+    (src, dst) and n."""
+    import torch
+    ta, tab, tabc = _rmat_thresholds(a, b, c)
+    n = 1 << scale
+    m = edge_factor << scale
+    base = _as_signed64(_rmat_key_base(seed) + _SM_GAMMA)
+    m1, m2 = _as_signed64(_SM_M1), _as_signed64(_SM_M2)
+
+    def lsr(z, k):
+        return (z >> k) & ((1 << (64 - k)) - 1)
+
+    src = torch.empty(m, dtype=torch.int32, device=device)
+    dst = torch.empty(m, dtype=torch.int32, device=device)
+    chunk = 1 << 24
+    for s0 in range(0, m, chunk):
+        e0 = min(m, s0 + chunk)
+        key0 = torch.arange(s0, e0, dtype=torch.int64, device=device) * 64 + base
+        u = torch.zeros(e0 - s0, dtype=torch.int64, device=device)
+        v = torch.zeros_like(u)
+        for lev in range(scale):
+            z = key0 + lev
+            z = (z ^ lsr(z, 30)) * m1
+            z = (z ^ lsr(z, 27)) * m2
+            z = z ^ lsr(z, 31)
+            x = lsr(z, 32)
+            row = x >= tab
+            col = ((x >= ta) & (x < tab)) | (x >= tabc)
+            u = (u << 1) | row.to(torch.int64)
+            v = (v << 1) | col.to(torch.int64)
+        src[s0:e0] = u.to(torch.int32)
+        dst[s0:e0] = v.to(torch.int32)
     return src, dst, n
 
 
@@ -236,22 +335,27 @@ def batch_mix_plan(num_graphs: int, n_min: int = 256, n_max: int = 65536, seed: 
 
 
 def batch_mix_device(num_graphs: int, n_min: int = 256, n_max: int = 65536, seed: int = 0,
-                     device="cuda"):
+                     device="cuda", select=None):
     """batch_mix generated on the GPU: the same kinds, sizes and distributions (plan from
     batch_mix_plan), the edges drawn by torch's seeded device generator (one per graph)
     straight into two int32 device arrays, so batches of billions of edges need no host
-    memory.  Returns (src, dst, offsets int64[G+1], num_vertices int32[G], kinds)."""
+    memory.  select (optional): indices of the graphs to generate, in that order; graph g
+    gets the same edges as in the whole mix.  Returns (src, dst, offsets int64[G+1],
+    num_vertices int32[G], kinds) over the generated graphs."""
     import torch
-    plan = batch_mix_plan(num_graphs, n_min, n_max, seed)
+    full = batch_mix_plan(num_graphs, n_min, n_max, seed)
+    which = list(range(num_graphs)) if select is None else [int(i) for i in select]
+    plan = [full[i] for i in which]
     sizes = [sum(sg[-1] for sg in segs) for _, _, segs in plan]
-    offsets = np.zeros(num_graphs + 1, np.int64)
+    offsets = np.zeros(len(plan) + 1, np.int64)
     offsets[1:] = np.cumsum(sizes)
     src = torch.empty(int(offsets[-1]), dtype=torch.int32, device=device)
     dst = torch.empty_like(src)
-    for g, (kind, n, segs) in enumerate(plan):
+    for gi, (kind, n, segs) in enumerate(plan):
+        g = which[gi]
+        a = int(offsets[gi])
         gen = torch.Generator(device=device)
         gen.manual_seed(int(seed) * 1_000_003 + g)
-        a = int(offsets[g])
         for sg in segs:
             if sg[0] == "rmat":
                 _, scale, m = sg

@@ -8,6 +8,7 @@ The tile counts and array digests come from the oracle's Bit-BSR builder (the
 reference's builder is GPU-only; the GPU tests compare the two on the device).
 
 Run from the repository root:  python tests/golden/make_golden.py
+(``--large`` writes golden_large.json instead: the full-size graphs, counts only.)
 """
 from __future__ import annotations
 
@@ -63,7 +64,45 @@ def digest(a: np.ndarray) -> str:
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()[:16]
 
 
+def large_specs():
+    """Full-size graphs (the R-MAT scale-22 headline graph and the served stream's large
+    requests), counted by the reference's CPU path; only counts and sizes are stored."""
+    return [
+        ("rmat_raw_22_16_s7", "rmat_raw_np", dict(scale=22, edge_factor=16, seed=7)),
+        ("rmat_raw_20_16_s21", "rmat_raw_np", dict(scale=20, edge_factor=16, seed=21)),
+        ("rmat_raw_18_16_s7", "rmat_raw_np", dict(scale=18, edge_factor=16, seed=7)),
+        ("stencil7_128", "stencil7", dict(k=128)),
+    ]
+
+
+def main_large():
+    if not O.ref_cpu_available():
+        O.build(ref=True)
+    threads = os.cpu_count() or 1
+    fixtures = {}
+    for name, gen, kw in large_specs():
+        src, dst, n = generate(gen, kw)
+        rpd, cold, _ = O.lower_csr(src, dst, n, "degree")
+        ref = int(O.ref_cpu_count(rpd, cold, threads))
+        entry = dict(generator=gen, kwargs=kw, n=int(n), m_input=int(len(src)),
+                     m_lower=int(len(cold)), count=ref,
+                     edges_digest=digest(np.stack([src, dst]).astype(np.int32)))
+        for C in (32, 128):
+            entry[f"tiles_{C}_degree"] = int(O.bitbsr_num_tiles(rpd, cold, n, C))
+        fixtures[name] = entry
+        print(f"{name:22s} n={n:8d} m={len(cold):9d} count={ref}", flush=True)
+    with open(os.path.join(OUT_DIR, "golden_large.json"), "w") as f:
+        json.dump(dict(
+            source="counts from the reference's cpu_tc_intersection_lower_triangular "
+                   "(oracle/_ref/libref_cpu.so) on the descending-degree lower CSR; tile "
+                   "counts from oracle/oracle.c",
+            fixtures=fixtures), f, indent=1, sort_keys=True)
+
+
 def main():
+    if "--large" in sys.argv[1:]:
+        main_large()
+        return
     if not O.ref_cpu_available():
         O.build(ref=True)
     fixtures = {}

@@ -1,7 +1,8 @@
 """GPU tests of the continuous-batching server (btc_server_*): every request's count is
-the same alone (plain path, and the single-graph BitBSR) and in the mix, whatever
-batch it lands in and however its arrival overlaps others on the device.  Counts are
-integers, so the tolerance is zero."""
+the reference CPU path's count of that graph (cpu_tc_intersection_lower_triangular,
+btc/operations/triangle_count_cpu.h:59-101), the same alone (plain path, and the
+single-graph BitBSR) and in the mix, whatever batch it lands in and however its arrival
+overlaps others on the device.  Counts are integers, so the tolerance is zero."""
 from __future__ import annotations
 
 import time
@@ -13,7 +14,13 @@ pytestmark = pytest.mark.gpu
 
 torch = pytest.importorskip("torch")
 
+import json  # noqa: E402
+import os  # noqa: E402
+
+from conftest import GOLDEN_DIR  # noqa: E402
+
 from btc_b200 import BitBSR, Server, graphs as G, _lib  # noqa: E402
+from oracle import oracle as O  # noqa: E402
 
 
 def _pool():
@@ -23,9 +30,23 @@ def _pool():
     return gs
 
 
+def _reference(gs):
+    """The reference CPU path's count of each graph (the oracle restatement where the
+    reference build is absent)."""
+    fn = O.ref_cpu_count if O.ref_cpu_available() else O.tc_merge
+    out = []
+    for s, d, n in gs:
+        rp, col, _ = O.lower_csr(s, d, n)
+        out.append(int(fn(rp, col, os.cpu_count() or 1)))
+    return out
+
+
 def _alone(gs):
-    return [BitBSR(torch.from_numpy(s).cuda(), torch.from_numpy(d).cuda(), n, 32).count()
-            for s, d, n in gs]
+    want = _reference(gs)
+    single = [BitBSR(torch.from_numpy(s).cuda(), torch.from_numpy(d).cuda(), n, 32).count()
+              for s, d, n in gs]
+    assert single == want
+    return want
 
 
 def _run(server, gs, order, gap_s=0.0, borrow=False):
@@ -89,3 +110,24 @@ def test_close_drains_queue():
     for s, d, n in gs:
         srv.submit(s, d, n)
     srv.close()  # returns after every queued request ran
+
+
+def test_large_requests_in_the_mix():
+    """The served workload's large requests (R-MAT scale 20 ef 16 and the 7-point stencil
+    128^3) among small ones: each large count equals its golden count, each small one the
+    reference CPU count, alone and in the mix."""
+    with open(os.path.join(GOLDEN_DIR, "golden_large.json")) as f:
+        fx = json.load(f)["fixtures"]
+    r20 = G.rmat_raw_np(**fx["rmat_raw_20_16_s21"]["kwargs"])
+    st7 = G.stencil7(128)
+    small = _pool()[:20]
+    gs = small + [r20, st7]
+    want = _reference(small) + [fx["rmat_raw_20_16_s21"]["count"], 0]
+    order = list(range(len(small))) + [len(small)] + list(range(len(small))) + [len(small) + 1] * 2
+    for slots, max_graphs in ((2, 4096), (1, 1)):
+        srv = Server(slots=slots, max_batch_graphs=max_graphs, tile_cols=32)
+        try:
+            for k, c in _run(srv, gs, order, gap_s=0.0002, borrow=True):
+                assert c == want[k], k
+        finally:
+            srv.close()
