@@ -122,7 +122,24 @@ struct BuildPlan {
     bool degree;
     uint64_t bm_words;
     uint32_t cap;  // > 0: the post-count steps run against this tile capacity
+    bool row_index = false;  // build the row-wise count's row index (rowindex.cu)
 };
+
+static bool row_index_possible(int64_t m, int32_t n_row_blocks)
+{
+    return n_row_blocks > 0 && m >= 8 * (int64_t)n_row_blocks && m < (int64_t)0xffffffffll;
+}
+
+// The row index after the row masks (T = *d_tiles bounded by cap, or cap itself).
+static int enqueue_row_index(btc_bitbsr* g, const unsigned long long* d_tiles, uint32_t cap,
+                             cudaStream_t s)
+{
+    unsigned long long* total = g->row_bsum.as<unsigned long long>();
+    return launch_rowindex(g->indptr.as<uint32_t>(), g->indices.as<uint32_t>(), g->n_row_blocks,
+                           g->rowmask.as<uint32_t>(), d_tiles, cap, g->row_tot.as<uint32_t>(),
+                           reinterpret_cast<uint32_t*>(total + 1), total, g->row_off.as<uint32_t>(),
+                           g->row_ent.as<uint2>(), g->row_ent.bytes / sizeof(uint2), s);
+}
 
 // Enqueues the build up to the tile count (bitmap path) or up to the tile segmentation
 // (radix path), and with plan.cap > 0 the whole bitmap build.  No waits, no allocation:
@@ -173,6 +190,7 @@ static int enqueue_build(btc_bitbsr* g, const BuildPlan& P, uint64_t** sorted_ou
             BTC_TRY(launch_rowmask(geom.tile_cols, g->blocks.as<uint32_t>(), P.cap,
                                    meta + kMetaTiles, g->indptr.as<uint32_t>(), geom.n_row_blocks,
                                    g->rowmask.as<uint32_t>(), meta + kMetaRowMax, s));
+            if (P.row_index) BTC_TRY(enqueue_row_index(g, meta + kMetaTiles, P.cap, s));
         }
     } else {
         // ---- keys, sort, segmentation ---------------------------------------
@@ -196,7 +214,8 @@ static void build_key(const btc_bitbsr* g, const BuildPlan& P, BuildGraphKey* k)
     const void* w[] = {P.src, P.dst, g->meta.ptr, g->in_src.ptr, g->in_dst.ptr, g->keys0.ptr,
                        g->keys1.ptr, g->sort_scratch.ptr, g->deg.ptr, g->rank.ptr, g->bitmap.ptr,
                        g->prefix.ptr, g->tile_base.ptr, g->indices.ptr, g->row_indices.ptr,
-                       g->indptr.ptr, g->blocks.ptr, g->rowmask.ptr, g->d_hmeta};
+                       g->indptr.ptr, g->blocks.ptr, g->rowmask.ptr, g->d_hmeta, g->row_off.ptr,
+                       g->row_ent.ptr, g->row_tot.ptr, g->row_bsum.ptr};
     static_assert(sizeof(w) / sizeof(w[0]) == kBuildKeyPtrs, "key layout");
     for (int i = 0; i < kBuildKeyPtrs; ++i) k->ptr[i] = w[i];
     k->m = P.m;
@@ -292,6 +311,7 @@ static int build_into(btc_bitbsr* g, const int32_t* src, const int32_t* dst, int
     P.use_bitmap = !(flags & BTC_BUILD_RADIX) && bm_bytes <= (4ull << 30) &&
                    bm_bytes <= 32ull * (uint64_t)m + (64ull << 20);
     g->used_bitmap = P.use_bitmap;
+    g->row_index = false;
     P.degree = (flags & BTC_ORIENT_DEGREE) && n > 0;
     size_t key_cap = P.use_bitmap ? 0 : (size_t)m;
     if (P.degree && (size_t)n > key_cap) key_cap = (size_t)n;
@@ -309,6 +329,18 @@ static int build_into(btc_bitbsr* g, const int32_t* src, const int32_t* dst, int
     if (P.use_bitmap) {
         BTC_TRY(g->bitmap.reserve(sizeof(uint32_t) * (P.bm_words ? P.bm_words : 1)));
         BTC_TRY(g->prefix.reserve(sizeof(uint2) * (P.bm_words ? P.bm_words : 1)));
+        // the row-wise count's row index: only a graph with at least 8 edges per row block
+        // can average 8 tiles per row block (every tile holds an edge)
+        P.row_index = row_index_possible(m, geom.n_row_blocks);
+        if (P.row_index) {
+            const uint64_t R = (uint64_t)geom.n_row_blocks;
+            BTC_TRY(g->row_off.reserve(sizeof(uint32_t) * (16 * R + 1)));
+            BTC_TRY(g->row_ent.reserve(sizeof(uint2) * (size_t)m));
+            BTC_TRY(g->row_tot.reserve(sizeof(uint32_t) * R));
+            BTC_TRY(g->row_bsum.reserve(sizeof(unsigned long long) +
+                                        sizeof(uint32_t) * ((size_t)ri_scan_blocks((uint32_t)R) + 1)));
+        }
+        g->row_index = P.row_index;
     }
     BTC_TRY(g->indptr.reserve(sizeof(uint32_t) * ((size_t)geom.n_row_blocks + 1)));
     BTC_TRY(ensure_count_scratch(g));
@@ -379,6 +411,7 @@ static int build_into(btc_bitbsr* g, const int32_t* src, const int32_t* dst, int
     BTC_TRY(launch_rowmask(tile_cols, g->blocks.as<uint32_t>(), g->num_tiles, nullptr,
                            g->indptr.as<uint32_t>(), g->n_row_blocks, g->rowmask.as<uint32_t>(),
                            meta + kMetaRowMax, s));
+    if (P.row_index) BTC_TRY(enqueue_row_index(g, nullptr, g->num_tiles, s));
     return BTC_OK;
 }
 
@@ -407,7 +440,9 @@ int count_handle(btc_bitbsr* g, int tau, cudaStream_t s, unsigned long long* d_o
                         g->used_bitmap ? g->prefix.as<uint2>() : nullptr,
                         bitmap_words_per_row(make_geom(g->n, g->tile_cols)),
                         g->meta.as<unsigned long long>() + kMetaRowMax, tile_begin, tile_end,
-                        build_meta, g->num_tiles);
+                        build_meta, g->num_tiles,
+                        g->used_bitmap && g->row_index ? g->row_off.as<uint32_t>() : nullptr,
+                        g->used_bitmap && g->row_index ? g->row_ent.as<uint2>() : nullptr);
 }
 
 int resolve_build(btc_bitbsr* g)

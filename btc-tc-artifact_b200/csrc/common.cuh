@@ -157,7 +157,8 @@ int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
                  const uint2* cellpp = nullptr,
                  uint64_t cell_wpr = 0, const unsigned long long* row_max = nullptr,
                  uint32_t tile_begin = 0, uint32_t tile_end = 0xffffffffu,
-                 const unsigned long long* build_meta = nullptr, uint32_t tiles_hint = 0);
+                 const unsigned long long* build_meta = nullptr, uint32_t tiles_hint = 0,
+                 const uint32_t* row_off = nullptr, const uint2* row_ent = nullptr);
 
 // rowmask[t] bit r = tile t's row r has a bit, for t < T = *d_tiles (T = cap when d_tiles
 // is null) when T >= 8 * n_row_blocks (the heavy count variant's condition), and
@@ -167,6 +168,17 @@ int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
 int launch_rowmask(int tile_cols, const uint32_t* blocks, uint32_t cap,
                    const unsigned long long* d_tiles, const uint32_t* indptr, int32_t n_row_blocks,
                    uint32_t* rowmask, unsigned long long* row_max, cudaStream_t s);
+
+// Row index of the row-wise count kernel (rowindex.cu): for vertex u, ent[off[u],
+// off[u+1]) lists (column block, tile) of the tiles whose row u % 16 holds a bit, in tile
+// order.  Built when the row masks are (T >= 8 * n_row_blocks, T = *d_tiles or cap);
+// tot: n_row_blocks words, bsum: ri_scan_blocks(n_row_blocks) words, total: one uint64 of
+// scratch; off: 16 * n_row_blocks + 1 words; ent: ent_cap entries (>= the unique edges).
+uint32_t ri_scan_blocks(uint32_t n_row_blocks);
+int launch_rowindex(const uint32_t* indptr, const uint32_t* indices, int32_t n_row_blocks,
+                    const uint32_t* rowmask, const unsigned long long* d_tiles, uint32_t cap,
+                    uint32_t* tot, uint32_t* bsum, unsigned long long* total, uint32_t* off,
+                    uint2* ent, uint64_t ent_cap, cudaStream_t s);
 
 // Device metadata slots of a build (uint64 each): valid keys, out-of-range flag, tile
 // count, unique edges, sort length, longest row-block list, tile-capacity overflow flag,

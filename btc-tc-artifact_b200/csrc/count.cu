@@ -38,9 +38,10 @@
 //  * Dense path: per slice, every match feeds mma.sync.m16n8k128.row.col.s32.b1.b1.s32
 //    .and.popc twice (16x16 popcount block), masked by the slice's bits.  16x32 tiles
 //    pack four matches into the 128-bit k dimension, as tc_16x32_mma_v6.h:72-154 does.
-#include "common.cuh"
+#include "count_common.cuh"
 
 #include <cstddef>
+#include <cstdlib>
 
 #include <atomic>
 
@@ -55,13 +56,6 @@ constexpr int kSmallList = 16; // lists this short are staged as lists, not bitm
 constexpr int kBmWords = 256;  // bitmap mode: graphs with at most 8192 column blocks
 constexpr int kMCap = 64;      // matches buffered per warp before a bit pass
 constexpr int kBCap = 512;     // mask-bit codes buffered per warp per bit pass
-
-template <int C>
-struct Cfg {
-    static constexpr int WPR = C / 32;       // words per tile row
-    static constexpr int TW = 16 * WPR;      // words per tile
-    static constexpr int JPT = C / 16;       // 16-row blocks covered by a tile's columns
-};
 
 template <int C>
 struct __align__(16) WarpSmem {
@@ -91,21 +85,6 @@ static_assert(offsetof(WarpSmem<128>, nS) % 16 == 0 && offsetof(WarpSmem<32>, nS
 static_assert(sizeof(WarpSmem<128>) % 16 == 0 && sizeof(WarpSmem<32>) % 16 == 0,
               "per-warp areas keep the 16-byte alignment of the first one");
 
-// global -> shared copies that complete in the background (cp.async, sm_80+); the issuing
-// lane waits with cp_async_wait_all, then a __syncwarp publishes the words to the warp.
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem)
-{
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem)
-{
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-
 // Row block I's column-block list as the search structure of the current tile.
 struct ARow {
     uint32_t start;  // indptr[I]
@@ -115,35 +94,6 @@ struct ARow {
     uint32_t words;  // bitmap mode: bitmap words in use
     int mode;        // 0: sorted list in shared memory, 1: bitmap, 2: sorted list in HBM
 };
-
-__device__ __forceinline__ void mma_b1(int32_t (&c)[4], uint32_t a0, uint32_t a1, uint32_t b0)
-{
-    asm volatile(
-        "mma.sync.aligned.m16n8k128.row.col.s32.b1.b1.s32.and.popc "
-        "{%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
-        : "+r"(c[0]), "+r"(c[1]), "+r"(c[2]), "+r"(c[3])
-        : "r"(a0), "r"(a1), "r"(b0));
-}
-
-// lower_bound of x in a[0, len)
-__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* a, uint32_t len, uint32_t x)
-{
-    uint32_t lo = 0, hi = len;
-    while (lo < hi) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (a[mid] < x) lo = mid + 1;
-        else hi = mid;
-    }
-    return lo;
-}
-
-// 16-bit slice j of tile row r.
-template <int C>
-__device__ __forceinline__ uint32_t slice_of(const uint32_t* S, int r, int j)
-{
-    constexpr int WPR = Cfg<C>::WPR;
-    return (S[r * WPR + ((16 * j) >> 5)] >> ((16 * j) & 31)) & 0xFFFFu;
-}
 
 // Bits 0, 2, 4, ... 30 of x, packed into bits 0..15.
 __device__ __forceinline__ uint32_t compress_even(uint32_t x)
@@ -344,20 +294,6 @@ __device__ __forceinline__ unsigned long long bit_pass(WarpSmem<C>& s, uint32_t 
     return acc;
 }
 
-// Adds the warp's partial count to graph g (one atomic per graph change per warp).
-// lane 0 keeps the flushed total, so the CTA reduction still sees every unit once.
-__device__ __forceinline__ void flush_graph(unsigned long long& acc, unsigned long long& acc_total,
-                                            unsigned long long* graph_counts, uint32_t g, int lane)
-{
-#pragma unroll
-    for (int d = 16; d > 0; d >>= 1) acc += __shfl_xor_sync(kFull, acc, d);
-    if (lane == 0 && g != 0xffffffffu) {
-        if (acc) atomicAdd(&graph_counts[g], acc);
-        acc_total += acc;
-    }
-    acc = 0;
-}
-
 template <int C, bool kHeavy>
 __global__ void __launch_bounds__(kThreads, 4)
 k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
@@ -549,12 +485,7 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
             A = stage_row<C>(s, indices, a0, a1 - a0, lane);
             curI = I;
             if (graph_counts) {
-                uint32_t lo = 0, hi = num_graphs;  // last g with graph_rows[g] <= I
-                while (hi - lo > 1) {
-                    const uint32_t mid = (lo + hi) >> 1;
-                    if (graph_rows[mid] <= I) lo = mid;
-                    else hi = mid;
-                }
+                const uint32_t lo = graph_of_row_block(graph_rows, num_graphs, I);
                 if (lo != g_cur) {
                     flush_graph(acc, acc_total, graph_counts, g_cur, lane);
                     g_cur = lo;
@@ -838,41 +769,7 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
     }
 
     // ---- int64 block tree + last-CTA reduction ------------------------------
-#pragma unroll
-    for (int d = 16; d > 0; d >>= 1) acc += __shfl_down_sync(kFull, acc, d);
-    if (lane == 0) s_red[warp] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned long long sum = 0;
-        for (int w = 0; w < kWarps; ++w) sum += s_red[w];
-        scr.partials[blockIdx.x] = sum;
-        __threadfence();
-        const unsigned prev = atomicAdd(scr.done, 1u);
-        s_last = (prev == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (s_last) {
-        __threadfence();
-        unsigned long long sum = 0;
-        for (uint32_t i = threadIdx.x; i < gridDim.x; i += kThreads) sum += __ldcg(&scr.partials[i]);
-#pragma unroll
-        for (int d = 16; d > 0; d >>= 1) sum += __shfl_down_sync(kFull, sum, d);
-        if (lane == 0) s_red[warp] = sum;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            unsigned long long total = 0;
-            for (int w = 0; w < kWarps; ++w) total += s_red[w];
-            if (build_failed) total = ~0ull;
-            *scr.result = total;
-            if (scr.result2) *scr.result2 = total;
-            if (scr.result_host) {
-                *reinterpret_cast<volatile unsigned long long*>(scr.result_host) = total;
-                __threadfence_system();
-            }
-            *scr.done = 0u;
-            *scr.work = 0ull;
-        }
-    }
+    finish_count<kThreads>(acc, scr, build_failed, s_red, &s_last);
 }
 
 }  // namespace
@@ -908,7 +805,8 @@ int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
                  const uint32_t* graph_rows, uint32_t num_graphs, unsigned long long* graph_counts,
                  const uint32_t* rowmask, const uint2* cellpp,
                  uint64_t cell_wpr, const unsigned long long* row_max, uint32_t tile_begin,
-                 uint32_t tile_end, const unsigned long long* build_meta, uint32_t tiles_hint)
+                 uint32_t tile_end, const unsigned long long* build_meta, uint32_t tiles_hint,
+                 const uint32_t* row_off, const uint2* row_ent)
 {
     // build_meta: num_tiles is a capacity bound and the kernel reads the device tile
     // count; the schedule and the variant follow tiles_hint (the previous build's count)
@@ -934,6 +832,18 @@ int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
         rowmask = nullptr;
         cellpp = nullptr;
     }
+    // Heavy graphs built through the cell bitmap, with a row index, take the row-wise
+    // kernel (count_rows.cu); BTC_COUNT_TILEWISE=1 keeps them on this one (a switch for
+    // comparing the two).
+    static const bool tilewise = [] {
+        const char* e = std::getenv("BTC_COUNT_TILEWISE");
+        return e && e[0] == '1';
+    }();
+    if (heavy && cellpp && row_off && row_ent && !tilewise)
+        return launch_count_rows(tile_cols, indptr, indices, row_indices, blocks, num_tiles, tile_begin,
+                                 tile_end, n_row_blocks, tau, (uint32_t)chunk_s, scr, graph_rows,
+                                 num_graphs, graph_counts, rowmask, cellpp, cell_wpr, row_off, row_ent,
+                                 build_meta, grid, s);
 #define BTC_LAUNCH_COUNT(CC, HH)                                                              \
     k_count<CC, HH><<<grid, kThreads, 0, s>>>(indptr, indices, row_indices, blocks, num_tiles, \
                                               tile_begin, tile_end, n_row_blocks, tau,         \

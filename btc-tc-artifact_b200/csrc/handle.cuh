@@ -5,7 +5,7 @@
 
 // Arguments and buffers of an enqueued build (a cached build graph replays only when
 // they are unchanged).
-constexpr int kBuildKeyPtrs = 19;
+constexpr int kBuildKeyPtrs = 23;
 struct BuildGraphKey {
     const void* ptr[kBuildKeyPtrs];
     int64_t m;
@@ -24,9 +24,13 @@ struct btc_bitbsr {
     int64_t input_edges = 0;
     // Bit-BSR arrays (reference layout)
     btc200::DevBuf indptr, indices, row_indices, blocks, result, rowmask;
+    // row index of the row-wise count kernel (rowindex.cu): per-vertex list offsets and
+    // (column block, tile) entries, plus the scan's scratch
+    btc200::DevBuf row_off, row_ent, row_tot, row_bsum;
     // build workspace
     btc200::DevBuf in_src, in_dst, keys0, keys1, sort_scratch, tile_base, meta, deg, rank, bitmap, prefix;
     bool used_bitmap = false;
+    bool row_index = false;  // the last build made the row index (its graph can be heavy)
     // count scratch
     btc200::DevBuf partials, done;
     unsigned long long* h_meta = nullptr;  // pinned and mapped, 8 slots
@@ -49,7 +53,8 @@ struct btc_bitbsr {
     {
         const btc200::DevBuf* all[] = {&indptr, &indices, &row_indices, &blocks, &result, &in_src, &in_dst,
                                &keys0, &keys1, &sort_scratch, &tile_base, &meta, &deg, &rank,
-                               &bitmap, &prefix, &partials, &done, &rowmask};
+                               &bitmap, &prefix, &partials, &done, &rowmask, &row_off, &row_ent,
+                               &row_tot, &row_bsum};
         size_t s = 0;
         for (const btc200::DevBuf* b : all) s += b->bytes;
         return s;
@@ -58,7 +63,8 @@ struct btc_bitbsr {
     {
         btc200::DevBuf* all[] = {&indptr, &indices, &row_indices, &blocks, &result, &in_src, &in_dst,
                          &keys0, &keys1, &sort_scratch, &tile_base, &meta, &deg, &rank,
-                         &bitmap, &prefix, &partials, &done, &rowmask};
+                         &bitmap, &prefix, &partials, &done, &rowmask, &row_off, &row_ent,
+                         &row_tot, &row_bsum};
         for (btc200::DevBuf* b : all) b->release();
         if (h_meta) cudaFreeHost(h_meta);
         h_meta = nullptr;
