@@ -39,6 +39,8 @@ EXPORTS = [
     "btc_hashorder_params",
     "btc_should_reorder",
     "btc_lite_select_tile_cols",
+    "btc_tile_policy_from_features",
+    "btc_select_tile_policy",
     "btc_build_bitbsr",
     "btc_rebuild_bitbsr",
     "btc_count",
@@ -151,6 +153,10 @@ def lib():
         L.btc_hashorder_params.argtypes = [C.c_int, vp, vp]
         L.btc_should_reorder.argtypes = [i32, i64, C.c_int, C.c_char_p]
         L.btc_lite_select_tile_cols.argtypes = [i64, i32, C.c_int]
+        L.btc_tile_policy_from_features.argtypes = [i64, i32, C.c_uint32, C.c_double,
+                                                    C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.btc_select_tile_policy.argtypes = [vp, vp, i64, i32, C.c_uint32, vp,
+                                             C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.btc_build_bitbsr.argtypes = [vp, vp, i64, i32, C.c_int, u32, vp, P(vp)]
         L.btc_rebuild_bitbsr.argtypes = [vp, vp, vp, i64, i32, C.c_int, u32, vp]
         L.btc_count.argtypes = [vp, C.c_int, vp, P(C.c_ulonglong), P(C.c_float)]

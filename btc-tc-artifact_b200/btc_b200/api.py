@@ -33,6 +33,7 @@ __all__ = [
     "convert_coo_to_bcsr_16x128_gpu", "convert_coo_to_bcsr_16x32_gpu",
     "count_triangles_16x128_adaptive", "count_triangles_16x32_adaptive",
     "preprocess_for_triangle_counting", "lite_select_tile_cols", "BitBSR", "default_tau",
+    "tile_policy", "tile_policy_from_features",
     "Batch", "Server",
 ]
 
@@ -303,6 +304,30 @@ def lite_select_tile_cols(nnz: int, num_rows: int, mode: int = 0) -> int:
 
 def default_tau(tile_cols: int) -> int:
     return int(lib().btc_default_tau(int(tile_cols)))
+
+
+def tile_policy_from_features(m: int, n: int, orient_degree: bool = False,
+                              locality: float = 0.0) -> tuple[int, int]:
+    """The engine's tile policy (btc_tile_policy_from_features): (tile_cols, tau) from the
+    edge count, vertex count, degree-ordering request and id locality."""
+    c, t = C.c_int(0), C.c_int(0)
+    flags = _lib.BTC_ORIENT_DEGREE if orient_degree else 0
+    check(lib().btc_tile_policy_from_features(int(m), int(n), flags, float(locality), C.byref(c),
+                                              C.byref(t)), "btc_tile_policy_from_features")
+    return int(c.value), int(t.value)
+
+
+def tile_policy(src, dst, n: int, orient_degree: bool = False, stream=None) -> tuple[int, int]:
+    """(tile_cols, tau) the engine picks for this edge list (btc_select_tile_policy; what
+    tile_cols=0 applies).  numpy arrays are sampled on the host, CUDA tensors on the GPU."""
+    sp, dp, m, flags, keep = _edge_ptrs(src, dst)
+    if orient_degree:
+        flags |= _lib.BTC_ORIENT_DEGREE
+    c, t = C.c_int(0), C.c_int(0)
+    check(lib().btc_select_tile_policy(sp, dp, m, int(n), flags, _stream_ptr(stream), C.byref(c),
+                                       C.byref(t)), "btc_select_tile_policy")
+    del keep
+    return int(c.value), int(t.value)
 
 
 # ---------------------------------------------------------------------------

@@ -12,9 +12,18 @@ times (default tau), printing the counts: a fixed target for profilers.
 ``autotune(src, dst, n)`` measures the tile width for one graph (both widths built and
 timed, counts cross-checked); ``tune.py --autotune`` prints it for the standard graphs
 next to the reference's BTC-Lite choice.
+
+``tune.py --sweep OUT.json`` measures the class sweep the engine's tile policy
+(csrc/policy.cu) was set from: 37 graphs over five families (Erdos-Renyi, 27- and 7-point
+stencils, R-MAT in natural and descending-degree order, 8-block SBMs, complete graphs),
+both widths, three taus (default, all b1 MMA, all sparse), build and count with the L2
+flushed before each; ``tune.py --table OUT.json`` prints the markdown table with the
+measured best width, BTC-Lite's pick and the engine policy's pick.
 """
 from __future__ import annotations
 
+import json
+import math
 import statistics
 import sys
 
@@ -142,7 +151,118 @@ def main() -> None:
             g.free()
 
 
+def sweep_specs():
+    """(name, generator, degree_order) of the policy sweep."""
+    from . import graphs as G
+    specs = []
+    for n in (4096, 16384, 65536, 262144):
+        for d in (8, 16, 32):
+            specs.append((f"er_{n}_{d}", lambda n=n, d=d: G.erdos_renyi(n, d, seed=5), False))
+    for k in (16, 32, 64):
+        specs.append((f"st27_{k}", lambda k=k: G.stencil27(k), False))
+    for k in (32, 64):
+        specs.append((f"st7_{k}", lambda k=k: G.stencil7(k), False))
+    for sc in (12, 14, 16, 18, 20):
+        for deg in (False, True):
+            specs.append((f"rmat{sc}{'_deg' if deg else ''}", lambda sc=sc: G.rmat_raw_np(sc, 16, 7), deg))
+    for n in (2048, 8192, 32768):
+        for p in (0.05, 0.1, 0.3):
+            specs.append((f"sbm_{n}_{p}", lambda n=n, p=p: G.sbm(n, 8, p, 0.001, seed=3), False))
+    for n in (256, 1024):
+        specs.append((f"K{n}", lambda n=n: G.complete(n), False))
+    return specs
+
+
+def sweep(reps: int = 5) -> list:
+    """Both widths x three taus on every sweep graph (L2 flushed before each timing)."""
+    import torch
+
+    from .api import BitBSR
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+
+    def ev_ms(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flush.zero_()
+        e0.record()
+        fn()
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    out = []
+    for name, gen, deg in sweep_specs():
+        s_, d_, n = gen()
+        src, dst = torch.from_numpy(s_).cuda(), torch.from_numpy(d_).cuda()
+        row = dict(name=name, n=int(n), m_in=int(src.numel()), degree_order=deg)
+        cnt = None
+        for C in (32, 128):
+            g = BitBSR(src, dst, n, C, orient_degree=deg)
+            c = g.count()
+            cnt = c if cnt is None else cnt
+            if c != cnt:
+                raise AssertionError(f"{name}: 16x{C} counted {c}, 16x32 {cnt}")
+            b = statistics.median([ev_ms(lambda: g.rebuild(src, dst, n, C, orient_degree=deg))
+                                   for _ in range(reps)])
+            res = {}
+            for tau in (-1, 0, 0x7FFFFFFF):
+                ts = []
+                for _ in range(reps):
+                    flush.zero_()
+                    cc, ms = g.count(tau=tau, timing=True)
+                    if cc != cnt:
+                        raise AssertionError(f"{name}: tau {tau} counted {cc}, expected {cnt}")
+                    ts.append(ms)
+                res[str(tau)] = statistics.median(ts)
+            row[f"c{C}"] = dict(build_ms=b, count_ms=res, tiles=g.num_tiles, m_lower=g.num_edges)
+            g.free()
+        row["count"] = cnt
+        out.append(row)
+        print(json.dumps(row), file=sys.stderr, flush=True)
+    return out
+
+
+def policy_table(rows) -> str:
+    """Markdown table of a sweep: measured best width, BTC-Lite's and the policy's picks."""
+    import numpy as np
+
+    from .api import lite_select_tile_cols, tile_policy
+    lines = ["| graph | n | unique edges | 16x32 build + count ms | 16x128 build + count ms | "
+             "best | BTC-Lite | policy |", "|---|---|---|---|---|---|---|---|"]
+    slow = {"lite": [], "policy": []}
+    gens = {nm: (gen, deg) for nm, gen, deg in sweep_specs()}
+    for r in rows:
+        t = {C: r[f"c{C}"]["build_ms"] + r[f"c{C}"]["count_ms"]["-1"] for C in (32, 128)}
+        best = min(t, key=t.get)
+        lite = lite_select_tile_cols(r["m_in"], r["n"])
+        gen, deg = gens[r["name"]]
+        s_, d_, n = gen()
+        pol = tile_policy(np.asarray(s_), np.asarray(d_), n, orient_degree=deg)[0]
+        slow["lite"].append(t[lite] / t[best])
+        slow["policy"].append(t[pol] / t[best])
+        fmt = lambda C: f"{r[f'c{C}']['build_ms']:.3f} + {r[f'c{C}']['count_ms']['-1']:.3f}"
+        mark = lambda C: f"16x{C}" + ("" if C == best else f" (+{100 * (t[C] / t[best] - 1):.0f}%)")
+        lines.append(f"| {r['name']} | {r['n']} | {r['c128']['m_lower']} | {fmt(32)} | {fmt(128)} | "
+                     f"16x{best} | {mark(lite)} | {mark(pol)} |")
+    gm = {k: math.exp(sum(math.log(x) for x in v) / len(v)) for k, v in slow.items()}
+    lines.append("")
+    lines.append(f"Slowdown against the measured best, geometric mean: BTC-Lite {gm['lite']:.3f}, "
+                 f"policy {gm['policy']:.3f}; worst: BTC-Lite {max(slow['lite']):.2f}, policy "
+                 f"{max(slow['policy']):.2f}; picks slower by more than 2%: BTC-Lite "
+                 f"{sum(x > 1.02 for x in slow['lite'])}, policy {sum(x > 1.02 for x in slow['policy'])} "
+                 f"of {len(rows)}.")
+    return "\n".join(lines)
+
+
 if __name__ == "__main__":
+    if len(sys.argv) > 2 and sys.argv[1] == "--sweep":
+        rows = sweep()
+        with open(sys.argv[2], "w") as f:
+            json.dump({"graphs": rows}, f, indent=1)
+        sys.exit(0)
+    if len(sys.argv) > 2 and sys.argv[1] == "--table":
+        with open(sys.argv[2]) as f:
+            print(policy_table(json.load(f)["graphs"]))
+        sys.exit(0)
     import os
     sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
     from btc_b200 import tune as _t

@@ -226,7 +226,28 @@ static int batch_build_into(btc_batch* b, const int32_t* src, const int32_t* dst
         if (num_vertices[i] < 0 || edge_offsets[i + 1] < edge_offsets[i]) return BTC_E_INVAL;
         n_sum += num_vertices[i];
     }
-    if (tile_cols == 0) tile_cols = btc_lite_select_tile_cols(m, (int32_t)(n_sum > 0x7fffffff ? 0x7fffffff : n_sum), 0);
+    if (tile_cols == 0) {
+        // the engine's tile policy over the whole batch (policy.cu), each sampled edge's
+        // locality measured against its own graph's size
+        double L = 0.0;
+        if (flags & BTC_INPUT_ON_HOST) {
+            BTC_TRY(policy_locality(src, dst, m, 0, true, edge_offsets, num_vertices, (uint32_t)G, s, &L));
+        } else if (m > 0) {
+            DevBuf tmp;
+            const size_t eb = sizeof(int64_t) * ((size_t)G + 1), nb = sizeof(int32_t) * (size_t)G;
+            int st = tmp.reserve(eb + nb);
+            if (st == BTC_OK && (cudaMemcpyAsync(tmp.ptr, edge_offsets, eb, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+                                 cudaMemcpyAsync(tmp.as<char>() + eb, num_vertices, nb, cudaMemcpyHostToDevice, s) != cudaSuccess))
+                st = BTC_E_CUDA;
+            if (st == BTC_OK)
+                st = policy_locality(src, dst, m, 0, false, tmp.as<int64_t>(),
+                                     reinterpret_cast<const int32_t*>(tmp.as<char>() + eb), (uint32_t)G, s, &L);
+            tmp.release();
+            BTC_TRY(st);
+        }
+        BTC_TRY(btc_tile_policy_from_features(m, (int32_t)(n_sum > 0x7fffffff ? 0x7fffffff : n_sum), 0, L,
+                                              &tile_cols, nullptr));
+    }
     if (tile_cols != 32 && tile_cols != 128) return BTC_E_INVAL;
     const int log2c = tile_cols == 128 ? 7 : 5;
 

@@ -64,7 +64,9 @@ using namespace btc200;
 
 // Engine's default dense/sparse switch.  A tile takes the binary tensor-core path
 // when its popcount exceeds tau.
-int default_tau(int tile_cols) { return tile_cols == 128 ? 512 : 64; }
+// Measured on sm_100a (policy.cu, the tau sweep): 16x128 tiles switch to the binary
+// tensor core above 1024 bits (half full), 16x32 tiles above 64 (the reference's value).
+int default_tau(int tile_cols) { return tile_cols == 128 ? 1024 : 64; }
 
 static constexpr uint64_t kMaxEdges = (1ull << 32) - (uint64_t)kSortTile;
 
@@ -272,7 +274,15 @@ static int build_into(btc_bitbsr* g, const int32_t* src, const int32_t* dst, int
     if (flags & ~(BTC_INPUT_ON_HOST | BTC_ORIENT_DEGREE | BTC_BUILD_RADIX | BTC_BUILD_ASYNC))
         return BTC_E_INVAL;
     if (g->pending) resolve_build(g);  // an enqueued build still owns the buffers
-    if (tile_cols == 0) tile_cols = btc_lite_select_tile_cols(m, n, 0);
+    if (tile_cols == 0) {
+        // the engine's tile policy (policy.cu); an enqueued rebuild keeps the handle's
+        // width so that it needs no wait
+        if ((flags & BTC_BUILD_ASYNC) && (g->tile_cols == 32 || g->tile_cols == 128))
+            tile_cols = g->tile_cols;
+        else
+            BTC_TRY(btc_select_tile_policy(src, dst, m, n, flags & (BTC_INPUT_ON_HOST | BTC_ORIENT_DEGREE),
+                                           s, &tile_cols, nullptr));
+    }
     if (tile_cols != 32 && tile_cols != 128) return BTC_E_INVAL;
     BTC_CUDA_TRY(cudaGetDevice(&g->device));
 

@@ -180,6 +180,12 @@ int launch_rowindex(const uint32_t* indptr, const uint32_t* indices, int32_t n_r
                     uint32_t* tot, uint32_t* bsum, unsigned long long* total, uint32_t* off,
                     uint2* ent, uint64_t ent_cap, cudaStream_t s);
 
+// Id locality of an edge list for the tile policy (policy.cu): sampled share of edges
+// with |u - v| < 128 over the share uniform ids would give.  e_off / nv (nullable): the
+// batch layout, each edge measured against its own graph's vertex count.
+int policy_locality(const int32_t* src, const int32_t* dst, int64_t m, int32_t n, bool on_host,
+                    const int64_t* e_off, const int32_t* nv, uint32_t G, cudaStream_t s, double* L);
+
 // Device metadata slots of a build (uint64 each): valid keys, out-of-range flag, tile
 // count, unique edges, sort length, longest row-block list, tile-capacity overflow flag,
 // and the chunk-scan ticket (CTAs of the chunk popcount that have finished).

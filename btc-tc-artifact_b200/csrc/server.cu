@@ -205,7 +205,7 @@ int launch_slot(btc_server* s, Slot& sl)
     const bool solo = G == 1 && sl.reqs[0].m >= s->cfg.solo_edges;
     if (solo) {
         // a large graph gains nothing from batching; descending-degree orientation keeps
-        // its hub rows short (BTC-Lite picks the tile width)
+        // its hub rows short (the engine's tile policy then picks 16x128)
         // Rebuilds are enqueued without a host wait (BTC_BUILD_ASYNC), so the engine
         // thread goes on filling the other slots; finish_solo checks the build's status.
         if (!sl.solo) {

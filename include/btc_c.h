@@ -149,6 +149,25 @@ BTC_API int btc_should_reorder(int32_t num_rows, int64_t nnz, int sm_version,
  * "avg degree nnz/rows < 15 or rows < 50000 -> 32, else 128". */
 BTC_API int btc_lite_select_tile_cols(int64_t nnz, int32_t num_rows, int mode);
 
+/* The engine's tile policy: tile width and tau per graph class, chosen from cheap
+ * features -- BTC_ORIENT_DEGREE in flags (power-law input ordered by degree: 16x128),
+ * the average degree 2m/n (>= 512: 16x32) and the id locality `locality` (the share of
+ * edges with |u - v| < 128 over the share uniform ids would give; >= 16: 16x128, else
+ * 16x32) -- set from a measured sweep of both widths over five graph families on a B200.
+ * No counterpart in the reference, whose policy is the fixed BTC-Lite rule above (kept
+ * as the baseline this policy beats).  Host only; *tau (nullable) receives the measured
+ * default tau of the chosen width. */
+BTC_API int btc_tile_policy_from_features(int64_t m, int32_t n, uint32_t flags, double locality,
+                                          int* tile_cols, int* tau);
+
+/* The same policy with the locality sampled from the edge list itself (65,536 evenly
+ * spaced edges): on the host for BTC_INPUT_ON_HOST arrays, else by one small kernel on
+ * `stream` followed by one wait (16 bytes of device scratch, allocated and freed here).
+ * btc_build_bitbsr and btc_batch_build apply it when tile_cols is 0.  No counterpart in
+ * the reference. */
+BTC_API int btc_select_tile_policy(const int32_t* src, const int32_t* dst, int64_t m, int32_t n,
+                                   uint32_t flags, btc_stream_t stream, int* tile_cols, int* tau);
+
 /* ======================================================================== */
 /* Stream-ordered engine surface                                             */
 /* ======================================================================== */
@@ -165,7 +184,8 @@ typedef struct btc_bitbsr_view {
 } btc_bitbsr_view;
 
 /* Builds the Bit-BSR of an edge list (src[i], dst[i]), i < m, on n vertices with
- * 16 x tile_cols tiles (tile_cols 32 or 128; 0 applies btc_lite_select_tile_cols).
+ * 16 x tile_cols tiles (tile_cols 32 or 128; 0 applies btc_select_tile_policy, and an
+ * asynchronous rebuild with 0 keeps the handle's current width).
  * Orientation to (max, min), self-loop removal and deduplication happen on the GPU.
  * With BTC_INPUT_ON_HOST the arrays are host memory and are copied on `stream`.
  * Synchronises `stream` once (to size the tile arrays, or at the end of a rebuild that
@@ -279,7 +299,8 @@ typedef struct btc_batch btc_batch; /* opaque, device-resident */
  * num_vertices are host arrays.  src/dst are device arrays, or host arrays with
  * BTC_INPUT_ON_HOST.  The batch is the block-diagonal union of the graphs (graph g's
  * vertex v is union vertex 16*R_<g + v, R_<g = row blocks of graphs 0..g-1), with one
- * tile width for all (32, 128, or 0 for the BTC-Lite policy on the totals).
+ * tile width for all (32, 128, or 0 for btc_select_tile_policy over the whole batch, each
+ * sampled edge's locality measured against its own graph's size).
  * Synchronises `stream` once. */
 BTC_API int btc_batch_build(const int32_t* src, const int32_t* dst, const int64_t* edge_offsets,
                             const int32_t* num_vertices, int32_t num_graphs, int tile_cols,
@@ -318,10 +339,10 @@ typedef struct btc_server_config {
     int32_t max_batch_graphs;  /* requests per batch (1: no batching) */
     int32_t slots;             /* batches in flight at once (1..8; 2 overlaps them) */
     int64_t max_batch_edges;   /* input edges per batch */
-    int tile_cols;             /* 32, 128, or 0 for the BTC-Lite policy per batch */
+    int tile_cols;             /* 32, 128, or 0 for the engine's tile policy per batch */
     int tau;                   /* dense/sparse switch, BTC_TAU_DEFAULT */
     int64_t solo_edges;        /* requests with at least this many edges run alone,
-                                  degree-ordered, with the BTC-Lite tile width */
+                                  degree-ordered, with the engine's tile policy */
 } btc_server_config;
 
 typedef struct btc_server_result {

@@ -58,7 +58,7 @@ def test_host_only_calls():
     assert L.btc_abi_version() >> 16 == 1
     assert L.btc_strerror(0) == b"ok"
     assert L.btc_strerror(_lib.BTC_E_RANGE) == b"vertex id out of range"
-    assert L.btc_default_tau(128) == 512 and L.btc_default_tau(32) == 64
+    assert L.btc_default_tau(128) == 1024 and L.btc_default_tau(32) == 64
 
 
 @pytest.mark.parametrize("nnz,rows,mode,want", [

@@ -36,3 +36,25 @@ def test_b1_mma_peak_is_measured():
     assert lib().btc_b1_mma_peak(None, 200, C.byref(ops)) == 0
     assert 1e13 < ops.value < 1e17  # binary ops per second: tens to thousands of Tops
     assert lib().btc_b1_mma_peak(None, 0, C.byref(ops)) != 0
+
+
+@pytest.mark.parametrize("cfg", ["er_16384_16", "stencil27_64", "rmat22_deg"])
+def test_policy_pick_is_the_measured_best(cfg):
+    """On the single-graph configurations (Erdos-Renyi 16384 / 16, the 27-point stencil
+    64^3, R-MAT scale 22 in descending-degree order) the engine's tile policy -- what
+    tile_cols=0 applies -- picks the width that measures fastest (build + count, both
+    widths built and counted, counts cross-checked)."""
+    from btc_b200 import graphs as G, tile_policy, tune
+    deg = cfg == "rmat22_deg"
+    if cfg == "er_16384_16":
+        s, d, n = G.erdos_renyi(16384, 16, seed=1)
+    elif cfg == "stencil27_64":
+        s, d, n = G.stencil27(64)
+    else:
+        s, d, n = G.rmat_raw_torch(22, 16, 7, device="cuda")
+    if isinstance(s, np.ndarray):
+        s, d = torch.from_numpy(s).cuda(), torch.from_numpy(d).cuda()
+    pick = tile_policy(s, d, n, orient_degree=deg)[0]
+    r = tune.autotune(s, d, n, orient_degree=deg, reps=3)
+    t = {C: v["build_ms"] + v["count_ms"] for C, v in r["table"].items()}
+    assert pick == r["tile_cols"], (cfg, pick, t)
