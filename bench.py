@@ -360,8 +360,11 @@ def batch_groups(off, limit):
 def run_batch(args, rank, world):
     """Batched workload: the mixed graphs generated on the GPU (several 10^9 edges at full
     size), counted in a few batch launches (one build + one count per group of at most
-    2^30 edges), against the plain path (one build + one count + one host sync per graph,
-    reusing one handle)."""
+    2^30 edges; consecutive groups alternate between two batch handles on two streams, so
+    one group's build overlaps the previous group's count), against the plain path (one
+    build + one count + one host sync per graph, reusing one handle).  Adds a breakdown
+    by graph kind (plain: per-graph device time summed by kind; batched: one batch run per
+    kind) and the largest graphs' share of the plain time."""
     import torch
     from btc_b200 import Batch, BitBSR, graphs as G
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
@@ -371,27 +374,34 @@ def run_batch(args, rank, world):
     torch.cuda.synchronize()
     gen_s = time.perf_counter() - t0
     m_raw = int(off[-1])
-    stream = torch.cuda.current_stream()
+    main = torch.cuda.current_stream()
+    side = torch.cuda.Stream()
+    streams = [main, side]
     tile = args.tile if args.tile is not None else 32
     groups = batch_groups(off, BATCH_GROUP_EDGES)
 
-    def group_args(g0, g1):
-        a, z = int(off[g0]), int(off[g1])
-        return dict(src=d_src[a:z], dst=d_dst[a:z], offsets=off[g0:g1 + 1] - a,
-                    num_vertices=nv[g0:g1], tile_cols=tile, stream=stream)
+    def group_args(g0, g1, src=d_src, dst=d_dst, offs=off, nvs=nv):
+        a, z = int(offs[g0]), int(offs[g1])
+        return dict(src=src[a:z], dst=dst[a:z], offsets=offs[g0:g1 + 1] - a,
+                    num_vertices=nvs[g0:g1], tile_cols=tile)
 
-    b = Batch(**group_args(*groups[0]))
+    handles = [Batch(**group_args(*groups[0]), stream=main)]
+    if len(groups) > 1:
+        handles.append(Batch(**group_args(*groups[1]), stream=side))
     counts = np.zeros(args.graphs, np.uint64)
     for gi, (g0, g1) in enumerate(groups):
-        if gi:
-            b.rebuild(**group_args(g0, g1))
-        counts[g0:g1] = b.count(stream=stream)
+        h = handles[gi % len(handles)]
+        h.rebuild(**group_args(g0, g1), stream=streams[gi % len(handles)])
+        counts[g0:g1] = h.count(stream=streams[gi % len(handles)])
     d_counts = torch.zeros(args.graphs, dtype=torch.int64, device="cuda")
 
-    def batched_step():
-        for g0, g1 in groups:
-            b.rebuild(**group_args(g0, g1))
-            b.count_async(d_counts[g0:].data_ptr(), stream=stream)
+    def batched_step(grps=groups, ga=group_args, out=d_counts):
+        side.wait_stream(main)
+        for gi, (g0, g1) in enumerate(grps):
+            h, st = handles[gi % len(handles)], streams[gi % len(handles)]
+            h.rebuild(**ga(g0, g1), stream=st)
+            h.count_async(out[g0:].data_ptr(), stream=st)
+        main.wait_stream(side)
 
     for _ in range(args.warmup):
         batched_step()
@@ -400,26 +410,73 @@ def run_batch(args, rank, world):
           for _ in range(args.steps)]
     with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
         for e0, e1 in ev:
-            e0.record(stream)
+            e0.record(main)
             batched_step()
-            e1.record(stream)
+            e1.record(main)
         torch.cuda.synchronize()
     t_batch = sum(e0.elapsed_time(e1) for e0, e1 in ev) / args.steps / 1e3
-    assert np.array_equal(d_counts.cpu().numpy().astype(np.uint64), counts)
+    if not np.array_equal(d_counts.cpu().numpy().astype(np.uint64), counts):
+        raise SystemExit("batched counts of the timed steps differ from the first pass")
 
-    # plain: one launch sequence and one host sync per graph
+    # plain: one launch sequence and one host sync per graph; device time per graph too
     g1_ = BitBSR(d_src[: max(int(off[1]), 1)], d_dst[: max(int(off[1]), 1)], int(nv[0]), tile)
     plain_counts = np.zeros(args.graphs, np.uint64)
+    per_graph_ms = np.zeros(args.graphs)
+    pev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.graphs)]
     torch.cuda.synchronize()
     tp0 = time.perf_counter()
     for i in range(args.graphs):
         a, z = int(off[i]), int(off[i + 1])
-        g1_.rebuild(d_src[a:z], d_dst[a:z], int(nv[i]), tile, stream=stream)
-        plain_counts[i] = g1_.count(stream=stream)
+        pev[i][0].record(main)
+        g1_.rebuild(d_src[a:z], d_dst[a:z], int(nv[i]), tile, stream=main)
+        plain_counts[i] = g1_.count(stream=main)
+        pev[i][1].record(main)
     torch.cuda.synchronize()
     t_plain = time.perf_counter() - tp0
+    for i, (e0, e1) in enumerate(pev):
+        per_graph_ms[i] = e0.elapsed_time(e1)
     g1_.free()
-    assert np.array_equal(plain_counts, counts), "batched and plain counts differ"
+    if not np.array_equal(plain_counts, counts):
+        raise SystemExit("batched and plain counts differ")
+
+    # breakdown by kind: plain device time by kind; each kind batched on its own
+    kinds_arr = np.array(kinds_list)
+    sizes = np.diff(off)
+    breakdown = {}
+    for k in ("er", "sbm", "rmat"):
+        idx = np.flatnonzero(kinds_arr == k)
+        if idx.size == 0:
+            continue
+        ks = torch.cat([d_src[int(off[i]):int(off[i + 1])] for i in idx])
+        kd = torch.cat([d_dst[int(off[i]):int(off[i + 1])] for i in idx])
+        koff = np.zeros(idx.size + 1, np.int64)
+        koff[1:] = np.cumsum(sizes[idx])
+        knv = nv[idx]
+        kgroups = batch_groups(koff, BATCH_GROUP_EDGES)
+        kcounts = torch.zeros(idx.size, dtype=torch.int64, device="cuda")
+        kga = lambda g0, g1: group_args(g0, g1, ks, kd, koff, knv)
+        batched_step(kgroups, kga, kcounts)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(main)
+        batched_step(kgroups, kga, kcounts)
+        e1.record(main)
+        e1.synchronize()
+        if not np.array_equal(kcounts.cpu().numpy().astype(np.uint64), counts[idx]):
+            raise SystemExit(f"batched counts of the {k} graphs differ")
+        kb = e0.elapsed_time(e1)
+        kp = float(per_graph_ms[idx].sum())
+        breakdown[k] = {"graphs": int(idx.size), "raw_edge_pairs": int(sizes[idx].sum()),
+                        "plain_device_ms": kp, "batched_ms": kb, "speedup": kp / kb if kb else None}
+        del ks, kd
+    top = np.argsort(-sizes)[: max(1, args.graphs // 20)]
+    breakdown["largest_5pct"] = {"graphs": int(top.size), "raw_edge_pairs": int(sizes[top].sum()),
+                                 "plain_device_ms": float(per_graph_ms[top].sum()),
+                                 "share_of_plain_device_time": float(per_graph_ms[top].sum() /
+                                                                     per_graph_ms.sum())}
+    breakdown["plain_device_ms_total"] = float(per_graph_ms.sum())
+    breakdown["plain_wall_ms_total"] = t_plain * 1e3
 
     # e2e: the leading graphs whose edges fit E2E_SAMPLE_EDGES (all of them when the batch
     # is that small), their edges in pinned host memory, H2D inside the step
@@ -431,19 +488,21 @@ def run_batch(args, rank, world):
     np_src, np_dst = h_src.numpy(), h_dst.numpy()
     host_counts = np.zeros(n_e2e, np.uint64)
     e2e = []
+    b = handles[0]
     for _ in range(max(1, min(args.steps, 5))):
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
+        e0.record(main)
         for g0, g1 in e_groups:
             a, z = int(off[g0]), int(off[g1])
             b.rebuild(src=np_src[a:z], dst=np_dst[a:z], offsets=off[g0:g1 + 1] - a,
-                      num_vertices=nv[g0:g1], tile_cols=tile, stream=stream)
-            host_counts[g0:g1] = b.count(stream=stream)
-        e1.record(stream)
+                      num_vertices=nv[g0:g1], tile_cols=tile, stream=main)
+            host_counts[g0:g1] = b.count(stream=main)
+        e1.record(main)
         e1.synchronize()
         e2e.append(e0.elapsed_time(e1) / 1e3)
-    assert np.array_equal(host_counts, counts[:n_e2e])
+    if not np.array_equal(host_counts, counts[:n_e2e]):
+        raise SystemExit("e2e batched counts differ")
     t_e2e = statistics.median(e2e)
     kinds = {k: kinds_list.count(k) for k in ("er", "sbm", "rmat")}
     line = {
@@ -455,13 +514,14 @@ def run_batch(args, rank, world):
                                f"log-uniform [256, {args.n_max}]", "graphs": args.graphs,
                    "kinds": kinds, "raw_edge_pairs": m_raw, "raw_edge_bytes": 8 * m_raw,
                    "batch_launches": len(groups), "edges_per_launch_max": BATCH_GROUP_EDGES,
-                   "tile": f"16x{tile}",
+                   "handles_streams": len(handles), "tile": f"16x{tile}",
                    "triangles_total": int(counts.sum()), "generation_s": round(gen_s, 1),
                    "parallelism": f"replica x{world}" if world > 1 else "single GPU"},
         "plain": {"value": world * args.graphs / t_plain, "unit": "graphs/s",
                   "what": "one rebuild + one count + one host sync per graph, one reused handle"},
         "speedup_vs_plain": t_plain / t_batch,
         "edges_per_s": world * m_raw / t_batch,
+        "breakdown": breakdown,
         "e2e": {"value": world * n_e2e / t_e2e, "unit": "graphs/s",
                 "h2d_bytes_per_step": 8 * m_e2e, "d2h_bytes_per_step": 8 * n_e2e + 24 * len(e_groups),
                 "sample": f"the first {n_e2e} graphs ({m_e2e} edge pairs) from pinned host memory"},

@@ -21,6 +21,8 @@
 #include <thrust/copy.h>
 #include <thrust/device_ptr.h>
 #include <thrust/iterator/counting_iterator.h>
+#include <thrust/iterator/zip_iterator.h>
+#include <thrust/sort.h>
 
 #include "btc_compat.hpp"
 
@@ -38,16 +40,31 @@ void convert_csr_to_coo(COO& coo, const CSR& csr)
     thrust::copy(csr.values.begin(), csr.values.end(), coo.values.begin());
 }
 
-// COO sorted by row -> CSR: row pointer r is the first entry of row r.
+// COO -> CSR: row pointer r is the first entry of row r.  A COO whose rows are not
+// sorted (the state a HashOrder relabel leaves it in) is converted from a copy sorted by
+// (row, column); the reference's version asserts sorted rows and aborts instead
+// (btc/utils/csr_helpers.h:24), so its -v check fails after a reorder while this one works.
 template <typename CSR, typename COO>
 void convert_coo_to_csr(CSR& csr, const COO& coo)
 {
     csr.resize(coo.num_rows, coo.num_cols, coo.num_entries);
     auto first = thrust::make_counting_iterator<decltype(coo.num_rows)>(0);
-    thrust::lower_bound(coo.row_indices.begin(), coo.row_indices.end(), first,
-                        first + coo.num_rows + 1, csr.row_pointers.begin());
-    thrust::copy(coo.column_indices.begin(), coo.column_indices.end(), csr.column_indices.begin());
-    thrust::copy(coo.values.begin(), coo.values.end(), csr.values.begin());
+    if (thrust::is_sorted(coo.row_indices.begin(), coo.row_indices.end())) {
+        thrust::lower_bound(coo.row_indices.begin(), coo.row_indices.end(), first,
+                            first + coo.num_rows + 1, csr.row_pointers.begin());
+        thrust::copy(coo.column_indices.begin(), coo.column_indices.end(), csr.column_indices.begin());
+        thrust::copy(coo.values.begin(), coo.values.end(), csr.values.begin());
+        return;
+    }
+    auto rows = coo.row_indices;  // copies in the COO's memory space
+    csr.column_indices = coo.column_indices;
+    csr.values = coo.values;
+    auto cv = thrust::make_zip_iterator(thrust::make_tuple(rows.begin(), csr.values.begin()));
+    thrust::stable_sort_by_key(csr.column_indices.begin(), csr.column_indices.end(), cv);
+    auto cv2 = thrust::make_zip_iterator(thrust::make_tuple(csr.column_indices.begin(), csr.values.begin()));
+    thrust::stable_sort_by_key(rows.begin(), rows.end(), cv2);
+    thrust::lower_bound(rows.begin(), rows.end(), first, first + coo.num_rows + 1,
+                        csr.row_pointers.begin());
 }
 
 namespace compat_detail {
