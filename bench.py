@@ -531,19 +531,6 @@ def run_batch(args, rank, world):
         print(json.dumps(line), flush=True)
 
 
-def raw_rmat(scale: int, edge_factor: int, seed: int):
-    """R-MAT draws without dedup (the builder removes duplicates and self-loops)."""
-    gr = np.random.default_rng(seed)
-    m = edge_factor << scale
-    u = np.zeros(m, np.int64)
-    v = np.zeros(m, np.int64)
-    for _ in range(scale):
-        r = gr.random(m, dtype=np.float32)
-        u = (u << 1) | (r >= 0.76)
-        v = (v << 1) | (((r >= 0.57) & (r < 0.76)) | (r >= 0.95))
-    return u.astype(np.int32), v.astype(np.int32), 1 << scale
-
-
 def serve_once(Server, cfg, pool, large, lam, n_req, seed, want, large_frac=0.05):
     """Poisson arrivals at rate lam (a large_frac share of large requests, the rest from
     the pool) into one server, after a warm-up that grows every slot's buffers; returns
@@ -562,6 +549,7 @@ def serve_once(Server, cfg, pool, large, lam, n_req, seed, want, large_frac=0.05
     got = 0
     while got < warm:
         got += len(srv.poll(wait_ms=100))
+    st0 = srv.stats()  # the measured stream's figures are differences from here
     ids = {}
     results = []
     done_flag = threading.Event()
@@ -594,8 +582,13 @@ def serve_once(Server, cfg, pool, large, lam, n_req, seed, want, large_frac=0.05
     edges = sum(r["m"] for r in results)
     return {"lambda": lam, "requests": n_req, "graphs_per_s": n_req / span,
             "edges_per_s": edges / span, "p50_ms": float(np.percentile(lat, 50) * 1e3),
-            "p99_ms": float(np.percentile(lat, 99) * 1e3), "batches": int(st["batches"]),
-            "peak_device_gb": st["peak_device_bytes"] / 1e9}
+            "p99_ms": float(np.percentile(lat, 99) * 1e3),
+            "batches": int(st["batches"] - st0["batches"]),
+            "peak_device_gb": st["peak_device_bytes"] / 1e9,
+            "solo_launches": int(st["solo_launches"] - st0["solo_launches"]),
+            "solo_stream_ms": float(st["solo_stream_ms"] - st0["solo_stream_ms"]),
+            "batch_stream_ms": float(st["batch_stream_ms"] - st0["batch_stream_ms"]),
+            "large_requests": sum(1 for r in results if ids[r["id"]][0] == "L")}
 
 
 def run_serve(args, rank, world):
@@ -609,14 +602,20 @@ def run_serve(args, rank, world):
         return (torch.from_numpy(np.ascontiguousarray(s_)).pin_memory().numpy(),
                 torch.from_numpy(np.ascontiguousarray(d_)).pin_memory().numpy(), n_)
 
-    pool = [pinned((s, d, n)) for s, d, n, _ in G.batch_mix(args.pool, 256, args.n_max, seed=13)]
-    large = [pinned(raw_rmat(20, 16, seed=21)), pinned(G.stencil7(128))]
-    want = {}
+    pool_args = dict(num_graphs=args.pool, n_min=256, n_max=args.n_max, seed=13)
+    pool = [pinned((s, d, n)) for s, d, n, _ in G.batch_mix(**pool_args)]
+    large = [pinned(G.rmat_raw_np(20, 16, 21)), pinned(G.stencil7(128))]
     tile = args.tile if args.tile is not None else 32
-    for kind, lst in (("S", pool), ("L", large)):
-        for k, (s_, d_, n_) in enumerate(lst):
-            want[(kind, k)] = BitBSR(torch.from_numpy(s_).cuda(), torch.from_numpy(d_).cuda(),
-                                     n_, tile).count()
+    # every served count is checked against the reference CPU path's count of the graph:
+    # the pool's from tests/golden/golden_serve.json (make_golden.py --serve), the large
+    # R-MAT's from golden_large.json, the 7-point stencil's is 0 (bipartite)
+    with open(os.path.join(GOLDEN, "golden_serve.json")) as f:
+        gs = json.load(f)
+    if gs["pool"] != pool_args:
+        raise SystemExit(f"golden_serve.json holds the pool {gs['pool']}, not {pool_args}")
+    want = {("S", k): int(c) for k, c in enumerate(gs["counts"])}
+    want[("L", 0)] = golden_count("rmat_raw_20_16_s21")
+    want[("L", 1)] = 0
     lams = [float(x) for x in args.rates.split(",")]
     modes = {"batched": dict(slots=2, max_batch_graphs=4096, tile_cols=tile,
                              hbm_budget_bytes=150 << 30),

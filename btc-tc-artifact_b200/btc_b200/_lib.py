@@ -113,7 +113,9 @@ class BtcServerResult(C.Structure):
 class BtcServerStats(C.Structure):
     _fields_ = [("batches", C.c_uint64), ("graphs", C.c_uint64), ("edges", C.c_uint64),
                 ("rejected", C.c_uint64), ("queued", C.c_uint64),
-                ("peak_device_bytes", C.c_uint64), ("now_s", C.c_double)]
+                ("peak_device_bytes", C.c_uint64), ("now_s", C.c_double),
+                ("solo_launches", C.c_uint64), ("solo_stream_ms", C.c_double),
+                ("batch_stream_ms", C.c_double)]
 
 
 BTC_SUBMIT_BORROW = 0x1

@@ -94,7 +94,12 @@ def standard_graphs(names=None):
     makers = {"stencil27_64": lambda: G.stencil27(64),
               "er_16384_16": lambda: G.erdos_renyi(16384, 16, seed=1),
               "rmat18_deg": lambda: G.rmat(18, 16, seed=7),
-              "rmat20_deg": lambda: G.rmat(20, 16, seed=7)}
+              "rmat20_deg": lambda: G.rmat(20, 16, seed=7),
+              # the counter-based draws of the bench's R-MAT workloads (raw: the builder
+              # dedups), generated on the GPU
+              "rmat_raw18_deg": lambda: G.rmat_raw_torch(18, 16, 7),
+              "rmat_raw20_deg": lambda: G.rmat_raw_torch(20, 16, 21),
+              "rmat_raw22_deg": lambda: G.rmat_raw_torch(22, 16, 7)}
     names = names or ["stencil27_64", "er_16384_16", "rmat18_deg"]
     return [(k, makers[k](), k.endswith("_deg")) for k in names]
 
@@ -104,8 +109,9 @@ def count_once(name: str, tile: int, reps: int) -> None:
 
     from .api import BitBSR
     [(_, (s, d, n), deg)] = standard_graphs([name])
-    g = BitBSR(torch.from_numpy(s).cuda(), torch.from_numpy(d).cuda(), n, tile,
-               orient_degree=deg)
+    if not isinstance(s, torch.Tensor):
+        s, d = torch.from_numpy(s).cuda(), torch.from_numpy(d).cuda()
+    g = BitBSR(s, d, n, tile, orient_degree=deg)
     print(name, f"16x{tile}", g.num_tiles, [g.count() for _ in range(reps)], flush=True)
     g.free()
 

@@ -20,6 +20,7 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <mutex>
@@ -76,6 +77,7 @@ struct PinnedBuf {
 
 struct Slot {
     cudaStream_t stream = nullptr;
+    cudaEvent_t start = nullptr;  // recorded before the slot's first copy
     cudaEvent_t done = nullptr;
     btc_batch* batch = nullptr;
     btc_bitbsr* solo = nullptr;  // large requests: one graph, descending-degree order
@@ -87,6 +89,7 @@ struct Slot {
     size_t device_bytes = 0;
     bool busy = false;
     bool solo_async = false;  // the solo handle's rebuild was enqueued without a wait
+    bool solo_launch = false; // the slot's current launch runs one request alone
 };
 
 }  // namespace
@@ -104,6 +107,12 @@ struct btc_server {
     bool stop = false;
     uint64_t next_id = 1;
     btc_server_stats stats{};
+    // Host-side allocation-failure injection (tests): the buffer reservations of
+    // launch_slot are numbered from 1 in the order the engine thread makes them, and
+    // those listed in BTC_SERVER_FAIL_RESERVE (comma-separated) report BTC_E_NOMEM
+    // without allocating.  Read once, at btc_server_create.
+    std::vector<uint64_t> fail_reserve;
+    uint64_t reserve_no = 0;
 
     double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
 };
@@ -145,6 +154,13 @@ void publish(btc_server* s, Slot& sl, int status)
     }
     s->stats.batches += 1;
     s->stats.graphs += sl.reqs.size();
+    if (status == BTC_OK) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, sl.start, sl.done) != cudaSuccess) cudaGetLastError();
+        const bool solo = sl.reqs.size() == 1 && sl.solo_launch;
+        (solo ? s->stats.solo_stream_ms : s->stats.batch_stream_ms) += ms;
+        s->stats.solo_launches += solo;
+    }
     for (const Request& q : sl.reqs) s->stats.edges += (uint64_t)q.m;
     sl.reqs.clear();
     sl.busy = false;
@@ -172,13 +188,21 @@ int launch_slot(btc_server* s, Slot& sl)
         if (q.m < kDirectCopyEdges) staged += q.m;
     }
     const int64_t m = sl.offsets.back();
-    int st = sl.h_src.reserve(sizeof(int32_t) * (size_t)(staged ? staged : 1));
-    if (st == BTC_OK) st = sl.h_dst.reserve(sizeof(int32_t) * (size_t)(staged ? staged : 1));
-    if (st == BTC_OK) st = sl.h_counts.reserve(sizeof(unsigned long long) * (size_t)G);
-    if (st == BTC_OK) st = sl.d_counts.reserve(sizeof(unsigned long long) * (size_t)G);
-    if (st == BTC_OK) st = sl.d_src.reserve(sizeof(int32_t) * (size_t)(m ? m : 1));
-    if (st == BTC_OK) st = sl.d_dst.reserve(sizeof(int32_t) * (size_t)(m ? m : 1));
+    // every reservation is numbered (fail_reserve injects an allocation failure)
+    auto reserve = [&](auto& buf, size_t bytes) -> int {
+        const uint64_t k = ++s->reserve_no;
+        if (std::find(s->fail_reserve.begin(), s->fail_reserve.end(), k) != s->fail_reserve.end())
+            return BTC_E_NOMEM;
+        return buf.reserve(bytes);
+    };
+    int st = reserve(sl.h_src, sizeof(int32_t) * (size_t)(staged ? staged : 1));
+    if (st == BTC_OK) st = reserve(sl.h_dst, sizeof(int32_t) * (size_t)(staged ? staged : 1));
+    if (st == BTC_OK) st = reserve(sl.h_counts, sizeof(unsigned long long) * (size_t)G);
+    if (st == BTC_OK) st = reserve(sl.d_counts, sizeof(unsigned long long) * (size_t)G);
+    if (st == BTC_OK) st = reserve(sl.d_src, sizeof(int32_t) * (size_t)(m ? m : 1));
+    if (st == BTC_OK) st = reserve(sl.d_dst, sizeof(int32_t) * (size_t)(m ? m : 1));
     if (st != BTC_OK) return st;
+    if (cudaEventRecord(sl.start, sl.stream) != cudaSuccess) return BTC_E_CUDA;
     int32_t* hs = static_cast<int32_t*>(sl.h_src.p);
     int32_t* hd = static_cast<int32_t*>(sl.h_dst.p);
     int32_t* ds = sl.d_src.as<int32_t>();
@@ -203,6 +227,7 @@ int launch_slot(btc_server* s, Slot& sl)
                          sl.stream) != cudaSuccess))
         return BTC_E_CUDA;
     const bool solo = G == 1 && sl.reqs[0].m >= s->cfg.solo_edges;
+    sl.solo_launch = solo;
     if (solo) {
         // a large graph gains nothing from batching; descending-degree orientation keeps
         // its hub rows short (the engine's tile policy then picks 16x128)
@@ -400,6 +425,15 @@ int btc_server_create(const btc_server_config* cfg, btc_server** out)
     if (!s) return BTC_E_NOMEM;
     s->cfg = *cfg;
     s->t0 = Clock::now();
+    if (const char* f = std::getenv("BTC_SERVER_FAIL_RESERVE")) {
+        for (const char* p = f; *p;) {
+            char* end = nullptr;
+            const unsigned long long k = std::strtoull(p, &end, 10);
+            if (end == p) break;
+            if (k) s->fail_reserve.push_back(k);
+            p = *end == ',' ? end + 1 : end;
+        }
+    }
     if (cudaGetDevice(&s->device) != cudaSuccess) {
         delete s;
         return BTC_E_CUDA;
@@ -407,10 +441,11 @@ int btc_server_create(const btc_server_config* cfg, btc_server** out)
     s->slots.resize((size_t)cfg->slots);
     for (Slot& sl : s->slots) {
         if (cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) != cudaSuccess ||
-            cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess) {
+            cudaEventCreate(&sl.start) != cudaSuccess || cudaEventCreate(&sl.done) != cudaSuccess) {
             cudaGetLastError();
             for (Slot& o : s->slots) {
                 if (o.stream) cudaStreamDestroy(o.stream);
+                if (o.start) cudaEventDestroy(o.start);
                 if (o.done) cudaEventDestroy(o.done);
             }
             delete s;
@@ -491,6 +526,7 @@ void btc_server_destroy(btc_server* s)
         sl.h_dst.release();
         sl.h_counts.release();
         if (sl.stream) cudaStreamDestroy(sl.stream);
+        if (sl.start) cudaEventDestroy(sl.start);
         if (sl.done) cudaEventDestroy(sl.done);
     }
     delete s;

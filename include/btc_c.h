@@ -359,6 +359,11 @@ typedef struct btc_server_result {
 typedef struct btc_server_stats {
     uint64_t batches, graphs, edges, rejected, queued, peak_device_bytes;
     double now_s;
+    /* launches that ran one large request alone (the single-graph path), and the
+     * stream time (first copy to the result's copy back, CUDA events) spent in those
+     * and in batches; slots overlap, so the two may add up to more than wall time */
+    uint64_t solo_launches;
+    double solo_stream_ms, batch_stream_ms;
 } btc_server_stats;
 
 /* Fills the defaults: 150 GB budget, 4096 graphs and 256M edges per batch, 2 slots,
@@ -369,6 +374,13 @@ BTC_API void btc_server_default_config(btc_server_config* cfg);
  * arrival order while the batch stays within the caps and all slots stay within the
  * budget; requests that arrive while batches are on the GPU join the next batch. */
 BTC_API int btc_server_create(const btc_server_config* cfg, btc_server** out);
+
+/* Host-side allocation-failure injection, for tests of the server's recovery: when the
+ * environment variable BTC_SERVER_FAIL_RESERVE holds comma-separated positive integers
+ * at btc_server_create, the server's buffer reservations (six per launched batch,
+ * numbered from 1 in the order the engine makes them) with those numbers report
+ * BTC_E_NOMEM without allocating.  The requests of that batch complete with status
+ * BTC_E_NOMEM; the server goes on with the next ones.  No GPU fault is involved. */
 
 /* Queues a request (host edge arrays; local ids in [0, n)).  Returns at once;
  * *id_out identifies the result.  The edges are copied on submit, or, with

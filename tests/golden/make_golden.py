@@ -8,7 +8,8 @@ The tile counts and array digests come from the oracle's Bit-BSR builder (the
 reference's builder is GPU-only; the GPU tests compare the two on the device).
 
 Run from the repository root:  python tests/golden/make_golden.py
-(``--large`` writes golden_large.json instead: the full-size graphs, counts only.)
+(``--large`` writes golden_large.json instead: the full-size graphs, counts only;
+``--serve`` writes golden_serve.json: the served stream's request pool, counts only.)
 """
 from __future__ import annotations
 
@@ -99,9 +100,35 @@ def main_large():
             fixtures=fixtures), f, indent=1, sort_keys=True)
 
 
+SERVE_POOL = dict(num_graphs=512, n_min=256, n_max=65536, seed=13)
+
+
+def main_serve():
+    """Per-graph counts of the served stream's request pool (graphs.batch_mix with
+    SERVE_POOL), by the reference's CPU path; bench.py checks every served result
+    against them."""
+    if not O.ref_cpu_available():
+        O.build(ref=True)
+    threads = os.cpu_count() or 1
+    pool = G.batch_mix(**SERVE_POOL)
+    counts, digests = [], []
+    for s_, d_, n, kind in pool:
+        rp, col, _ = O.lower_csr(s_, d_, n)
+        counts.append(int(O.ref_cpu_count(rp, col, threads)))
+        digests.append(digest(np.stack([s_, d_]).astype(np.int32)))
+    with open(os.path.join(OUT_DIR, "golden_serve.json"), "w") as f:
+        json.dump(dict(source="counts from the reference's cpu_tc_intersection_lower_triangular "
+                              "(oracle/_ref/libref_cpu.so) of graphs.batch_mix(**pool)",
+                       pool=SERVE_POOL, counts=counts, edges_digests=digests), f)
+    print(len(counts), "graphs,", sum(counts), "triangles")
+
+
 def main():
     if "--large" in sys.argv[1:]:
         main_large()
+        return
+    if "--serve" in sys.argv[1:]:
+        main_serve()
         return
     if not O.ref_cpu_available():
         O.build(ref=True)

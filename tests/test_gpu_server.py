@@ -131,3 +131,29 @@ def test_large_requests_in_the_mix():
                 assert c == want[k], k
         finally:
             srv.close()
+
+
+def test_server_recovers_from_injected_allocation_failures(monkeypatch):
+    """Reservations 2 and 9 report BTC_E_NOMEM.  Reservations are numbered as they are
+    attempted (six per launched batch, none after a failure): request 0 fails at its
+    second (#2), request 1 takes #3-#8, request 2 fails at its first (#9).  Those two
+    complete with BTC_E_NOMEM and count 0; every other request, before and after, gets the
+    reference CPU count."""
+    gs = _pool()[:8]
+    want = _reference(gs)
+    monkeypatch.setenv("BTC_SERVER_FAIL_RESERVE", "2,9")
+    srv = Server(slots=1, max_batch_graphs=1)
+    monkeypatch.delenv("BTC_SERVER_FAIL_RESERVE")
+    try:
+        for k, (s, d, n) in enumerate(gs):  # one at a time: six reservations per request
+            rid = srv.submit(s, d, n)
+            res = []
+            while not res:
+                res = srv.poll(wait_ms=200)
+            assert res[0]["id"] == rid
+            if k in (0, 2):
+                assert res[0]["status"] == _lib.BTC_E_NOMEM and res[0]["count"] == 0, res
+            else:
+                assert res[0]["status"] == 0 and res[0]["count"] == want[k], (k, res)
+    finally:
+        srv.close()
