@@ -275,13 +275,16 @@ static int build_into(btc_bitbsr* g, const int32_t* src, const int32_t* dst, int
         return BTC_E_INVAL;
     if (g->pending) resolve_build(g);  // an enqueued build still owns the buffers
     if (tile_cols == 0) {
-        // the engine's tile policy (policy.cu); an enqueued rebuild keeps the handle's
-        // width so that it needs no wait
-        if ((flags & BTC_BUILD_ASYNC) && (g->tile_cols == 32 || g->tile_cols == 128))
+        // the engine's tile policy (policy.cu).  With degree ordering it needs only m and
+        // n; otherwise it samples the edges (a wait), which an enqueued rebuild skips by
+        // keeping the handle's width.
+        if (flags & BTC_ORIENT_DEGREE)
+            BTC_TRY(btc_tile_policy_from_features(m, n, BTC_ORIENT_DEGREE, 0.0, &tile_cols, nullptr));
+        else if ((flags & BTC_BUILD_ASYNC) && (g->tile_cols == 32 || g->tile_cols == 128))
             tile_cols = g->tile_cols;
         else
-            BTC_TRY(btc_select_tile_policy(src, dst, m, n, flags & (BTC_INPUT_ON_HOST | BTC_ORIENT_DEGREE),
-                                           s, &tile_cols, nullptr));
+            BTC_TRY(btc_select_tile_policy(src, dst, m, n, flags & BTC_INPUT_ON_HOST, s, &tile_cols,
+                                           nullptr));
     }
     if (tile_cols != 32 && tile_cols != 128) return BTC_E_INVAL;
     BTC_CUDA_TRY(cudaGetDevice(&g->device));

@@ -5,11 +5,11 @@
 // The rule comes from a sweep on one B200 of 37 graphs over five families (Erdos-Renyi,
 // 27- and 7-point stencils, R-MAT in natural and descending-degree order, 8-block SBMs,
 // complete graphs) at both tile widths and three taus (btc_b200/tune.py --sweep; table in
-// the autotune profile).  Features, all cheap:
-//   * descending-degree order requested (BTC_ORIENT_DEGREE): power-law graphs whose hubs
-//     sit in the first column blocks -> 16x128;
+// the autotune profile).  Features, all cheap, in this order:
 //   * average degree d = 2m/n >= 512 (dense communities, near-cliques): 16x32, whose
 //     dense path packs four matches into one k = 128 MMA;
+//   * descending-degree order requested (BTC_ORIENT_DEGREE): power-law graphs whose hubs
+//     sit in the first column blocks -> 16x128;
 //   * id locality L: the share of sampled input edges with |u - v| < 128 over the share
 //     uniform ids would give (about 255/n); L >= 16 (banded or clustered ids: stencils)
 //     -> 16x128, else (random ids: Erdos-Renyi, natural-order R-MAT, SBM) 16x32.
@@ -134,8 +134,8 @@ int btc_tile_policy_from_features(int64_t m, int32_t n, uint32_t flags, double l
     if (m < 0 || n < 0 || !tile_cols) return BTC_E_INVAL;
     const double d = n > 0 ? 2.0 * (double)m / (double)n : 0.0;
     int C;
-    if (flags & BTC_ORIENT_DEGREE) C = 128;
-    else if (d >= 512.0) C = 32;
+    if (d >= 512.0) C = 32;
+    else if (flags & BTC_ORIENT_DEGREE) C = 128;
     else C = locality >= 16.0 ? 128 : 32;
     *tile_cols = C;
     if (tau) *tau = default_tau(C);

@@ -387,12 +387,24 @@ void engine_loop(btc_server* s)
             }
         }
         if (!launched) {
-            // every slot busy, or the next request must wait for memory: wait for a slot
-            for (Slot& sl : s->slots)
-                if (sl.busy) {
-                    cudaEventSynchronize(sl.done);
-                    break;
+            // every slot busy, or the next request must wait for memory: wait until any
+            // busy slot finishes (polling all of them, so a short batch on one slot is
+            // published while a long one still runs on another)
+            for (;;) {
+                bool any_busy = false, any_done = false;
+                for (Slot& sl : s->slots) {
+                    if (!sl.busy) continue;
+                    any_busy = true;
+                    const cudaError_t q = cudaEventQuery(sl.done);
+                    if (q == cudaSuccess) any_done = true;
+                    else if (q != cudaErrorNotReady) {
+                        cudaGetLastError();
+                        any_done = true;  // publish reports the slot's failure
+                    }
                 }
+                if (!any_busy || any_done) break;
+                std::this_thread::sleep_for(std::chrono::microseconds(20));
+            }
         }
     }
 }

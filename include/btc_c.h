@@ -150,10 +150,11 @@ BTC_API int btc_should_reorder(int32_t num_rows, int64_t nnz, int sm_version,
 BTC_API int btc_lite_select_tile_cols(int64_t nnz, int32_t num_rows, int mode);
 
 /* The engine's tile policy: tile width and tau per graph class, chosen from cheap
- * features -- BTC_ORIENT_DEGREE in flags (power-law input ordered by degree: 16x128),
- * the average degree 2m/n (>= 512: 16x32) and the id locality `locality` (the share of
- * edges with |u - v| < 128 over the share uniform ids would give; >= 16: 16x128, else
- * 16x32) -- set from a measured sweep of both widths over five graph families on a B200.
+ * features, in order -- the average degree 2m/n (>= 512: 16x32), BTC_ORIENT_DEGREE in
+ * flags (power-law input ordered by degree: 16x128) and the id locality `locality` (the
+ * share of edges with |u - v| < 128 over the share uniform ids would give; >= 16: 16x128,
+ * else 16x32) -- set from a measured sweep of both widths over five graph families on a
+ * B200.
  * No counterpart in the reference, whose policy is the fixed BTC-Lite rule above (kept
  * as the baseline this policy beats).  Host only; *tau (nullable) receives the measured
  * default tau of the chosen width. */
@@ -184,8 +185,9 @@ typedef struct btc_bitbsr_view {
 } btc_bitbsr_view;
 
 /* Builds the Bit-BSR of an edge list (src[i], dst[i]), i < m, on n vertices with
- * 16 x tile_cols tiles (tile_cols 32 or 128; 0 applies btc_select_tile_policy, and an
- * asynchronous rebuild with 0 keeps the handle's current width).
+ * 16 x tile_cols tiles (tile_cols 32 or 128; 0 applies btc_select_tile_policy -- an
+ * asynchronous rebuild of an edge list not ordered by degree keeps the handle's current
+ * width instead, since the policy's edge sample would wait).
  * Orientation to (max, min), self-loop removal and deduplication happen on the GPU.
  * With BTC_INPUT_ON_HOST the arrays are host memory and are copied on `stream`.
  * Synchronises `stream` once (to size the tile arrays, or at the end of a rebuild that

@@ -20,8 +20,9 @@ def test_rules():
     assert tile_policy_from_features(10 ** 6, 10 ** 5, orient_degree=True) == (128, 1024)
     assert tile_policy_from_features(10 ** 6, 10 ** 5, locality=1.0) == (32, 64)
     assert tile_policy_from_features(10 ** 6, 10 ** 5, locality=16.0) == (128, 1024)
-    # average degree >= 512: 16x32 whatever the locality
+    # average degree >= 512: 16x32 whatever the locality or the ordering
     assert tile_policy_from_features(300 * 1000, 1000, locality=100.0) == (32, 64)
+    assert tile_policy_from_features(300 * 1000, 1000, orient_degree=True) == (32, 64)
     assert tile_policy_from_features(0, 0) == (32, 64)
 
 
@@ -35,7 +36,7 @@ def test_rules():
 def test_host_sample(gen, want):
     s, d, n = gen()
     assert tile_policy(s, d, n)[0] == want
-    assert tile_policy(s, d, n, orient_degree=True)[0] == 128
+    assert tile_policy(s, d, n, orient_degree=True)[0] == (32 if 2 * len(s) >= 512 * n else 128)
 
 
 def _sweep():
