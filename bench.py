@@ -360,11 +360,11 @@ def batch_groups(off, limit):
 def run_batch(args, rank, world):
     """Batched workload: the mixed graphs generated on the GPU (several 10^9 edges at full
     size), counted in a few batch launches (one build + one count per group of at most
-    2^30 edges; consecutive groups alternate between two batch handles on two streams, so
-    one group's build overlaps the previous group's count), against the plain path (one
-    build + one count + one host sync per graph, reusing one handle).  Adds a breakdown
-    by graph kind (plain: per-graph device time summed by kind; batched: one batch run per
-    kind) and the largest graphs' share of the plain time."""
+    2^30 edges, one batch handle per group; a step -- every group's rebuild, enqueued
+    without a wait, and its count -- is one replayed CUDA graph), against the plain path
+    (one build + one count + one host sync per graph, reusing one handle).  Adds a
+    breakdown by graph kind (plain: per-graph device time summed by kind; batched: one
+    batch run per kind) and the largest graphs' share of the plain time."""
     import torch
     from btc_b200 import Batch, BitBSR, graphs as G
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
@@ -385,38 +385,75 @@ def run_batch(args, rank, world):
         return dict(src=src[a:z], dst=dst[a:z], offsets=offs[g0:g1 + 1] - a,
                     num_vertices=nvs[g0:g1], tile_cols=tile)
 
-    handles = [Batch(**group_args(*groups[0]), stream=main)]
-    if len(groups) > 1:
-        handles.append(Batch(**group_args(*groups[1]), stream=side))
+    # One batch handle per group (each keeps its group's arrays), all on one stream: a step
+    # enqueues every group's rebuild without a wait (same graphs' sizes as the first build)
+    # and its count, so the whole step is captured once as a CUDA graph and replayed.
+    ghandles = [Batch(**group_args(g0, g1), stream=main) for g0, g1 in groups]
     counts = np.zeros(args.graphs, np.uint64)
-    for gi, (g0, g1) in enumerate(groups):
-        h = handles[gi % len(handles)]
-        h.rebuild(**group_args(g0, g1), stream=streams[gi % len(handles)])
-        counts[g0:g1] = h.count(stream=streams[gi % len(handles)])
+    for h, (g0, g1) in zip(ghandles, groups):
+        counts[g0:g1] = h.count(stream=main)
     d_counts = torch.zeros(args.graphs, dtype=torch.int64, device="cuda")
 
-    def batched_step(grps=groups, ga=group_args, out=d_counts):
-        side.wait_stream(main)
-        for gi, (g0, g1) in enumerate(grps):
-            h, st = handles[gi % len(handles)], streams[gi % len(handles)]
-            h.rebuild(**ga(g0, g1), stream=st)
-            h.count_async(out[g0:].data_ptr(), stream=st)
-        main.wait_stream(side)
+    def enqueue_step(st):
+        for h, (g0, g1) in zip(ghandles, groups):
+            h.rebuild(**group_args(g0, g1), stream=st, asynchronous=True)
+            h.count_async(d_counts[g0:].data_ptr(), stream=st)
+
+    cap_stream = torch.cuda.Stream()
+    cap_stream.wait_stream(main)
+    enqueue_step(cap_stream)  # one enqueued step before capture
+    cap_stream.synchronize()
+    step_graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(step_graph, stream=cap_stream):
+        enqueue_step(cap_stream)
+
+    def batched_step_graph():
+        cap_stream.wait_stream(main)
+        with torch.cuda.stream(cap_stream):
+            step_graph.replay()
+        main.wait_stream(cap_stream)
 
     for _ in range(args.warmup):
-        batched_step()
+        batched_step_graph()
     torch.cuda.synchronize()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(args.steps)]
     with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
         for e0, e1 in ev:
             e0.record(main)
-            batched_step()
+            batched_step_graph()
             e1.record(main)
         torch.cuda.synchronize()
     t_batch = sum(e0.elapsed_time(e1) for e0, e1 in ev) / args.steps / 1e3
     if not np.array_equal(d_counts.cpu().numpy().astype(np.uint64), counts):
         raise SystemExit("batched counts of the timed steps differ from the first pass")
+    for h in ghandles:
+        h.count(stream=main)  # the enqueued builds' status (raises on a failure)
+    # the same step enqueued call by call (no graph), for comparison
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(main)
+    enqueue_step(main)
+    e1.record(main)
+    e1.synchronize()
+    t_enqueued = e0.elapsed_time(e1) / 1e3
+    for h in ghandles:
+        h.count(stream=main)
+        h.free()
+    del step_graph
+
+    # two handles alternating over varying groups (waiting rebuilds): the per-kind runs
+    handles = [Batch(**group_args(*groups[0]), stream=main)]
+    if len(groups) > 1:
+        handles.append(Batch(**group_args(*groups[1]), stream=side))
+
+    def batched_step(grps, ga, out):
+        side.wait_stream(main)
+        for gi, (g0, g1) in enumerate(grps):
+            h, st = handles[gi % len(handles)], streams[gi % len(handles)]
+            h.rebuild(**ga(g0, g1), stream=st)
+            h.count_async(out[g0:].data_ptr(), stream=st)
+        main.wait_stream(side)
 
     # plain: one launch sequence and one host sync per graph; device time per graph too
     g1_ = BitBSR(d_src[: max(int(off[1]), 1)], d_dst[: max(int(off[1]), 1)], int(nv[0]), tile)
@@ -514,12 +551,14 @@ def run_batch(args, rank, world):
                                f"log-uniform [256, {args.n_max}]", "graphs": args.graphs,
                    "kinds": kinds, "raw_edge_pairs": m_raw, "raw_edge_bytes": 8 * m_raw,
                    "batch_launches": len(groups), "edges_per_launch_max": BATCH_GROUP_EDGES,
-                   "handles_streams": len(handles), "tile": f"16x{tile}",
+                   "step": "one CUDA graph: every group's enqueued rebuild and count",
+                   "tile": f"16x{tile}",
                    "triangles_total": int(counts.sum()), "generation_s": round(gen_s, 1),
                    "parallelism": f"replica x{world}" if world > 1 else "single GPU"},
         "plain": {"value": world * args.graphs / t_plain, "unit": "graphs/s",
                   "what": "one rebuild + one count + one host sync per graph, one reused handle"},
         "speedup_vs_plain": t_plain / t_batch,
+        "enqueued_without_graph_ms": t_enqueued * 1e3,
         "edges_per_s": world * m_raw / t_batch,
         "breakdown": breakdown,
         "e2e": {"value": world * n_e2e / t_e2e, "unit": "graphs/s",
@@ -876,7 +915,13 @@ def main():
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": traffic,
                      "traffic_source": prof["source"] if prof else None,
-                     "kernel": f"k_count<{tile}>", "algorithmic_bytes": bytes_count,
+                     # DRAM bytes the launch really moves (ncu) over its live duration:
+                     # how close the kernel runs to the HBM bound its random sector
+                     # traffic sets
+                     "traffic_gbs": traffic / tc / 1e9 if traffic else None,
+                     "traffic_frac": traffic / tc / 1e9 / hbm if traffic else None,
+                     "kernel": prof["kernel"] if prof else f"k_count<{tile}>",
+                     "algorithmic_bytes": bytes_count,
                      "kernel_ms": tc * 1e3, "peak_source": peak_src},
         "issue": issue,
         "phases": {"count_ms": tc * 1e3, "build_ms": tb * 1e3,

@@ -479,12 +479,15 @@ class Batch:
         dst = np.concatenate(dsts) if dsts else np.zeros(0, np.int32)
         return src, dst, offsets, nv
 
-    def _build(self, fn, graphs, tile_cols, stream, src, dst, offsets, num_vertices, first):
+    def _build(self, fn, graphs, tile_cols, stream, src, dst, offsets, num_vertices, first,
+               asynchronous=False):
         if graphs is not None:
             src, dst, offsets, num_vertices = Batch.concat(graphs)
         offsets = np.ascontiguousarray(offsets, np.int64)
         num_vertices = np.ascontiguousarray(num_vertices, np.int32)
         sp, dp, m, flags, keep = _edge_ptrs(src, dst)
+        if asynchronous:
+            flags |= _lib.BTC_BUILD_ASYNC
         if m != int(offsets[-1]):
             raise BtcError(_lib.BTC_E_INVAL, "offsets[-1] != number of edges")
         self.num_graphs = len(num_vertices)
@@ -494,12 +497,17 @@ class Batch:
             check(fn(*args, C.byref(self._h)), "btc_batch_build")
         else:
             check(fn(self._h, *args), "btc_batch_rebuild")
-        del keep
+        # an enqueued build reads the edges after this call returns
+        self._keep = keep if asynchronous else None
 
     def rebuild(self, graphs=None, tile_cols: int = 0, stream=None, *, src=None, dst=None,
-                offsets=None, num_vertices=None) -> None:
+                offsets=None, num_vertices=None, asynchronous: bool = False) -> None:
+        """asynchronous=True enqueues the rebuild without host work or a wait when the graphs'
+        sizes equal the last build's and the edges are on the device (btc_batch_rebuild with
+        BTC_BUILD_ASYNC); its status comes with the next waiting call.  The edge tensors
+        must outlive the enqueued build."""
         self._build(lib().btc_batch_rebuild, graphs, tile_cols, stream, src, dst, offsets,
-                    num_vertices, first=False)
+                    num_vertices, first=False, asynchronous=asynchronous)
 
     def count(self, tau: int = _lib.BTC_TAU_DEFAULT, stream=None) -> np.ndarray:
         """Per-graph triangle counts (uint64 numpy array); waits for them."""

@@ -260,16 +260,16 @@ def policy_table(rows) -> str:
 
 
 if __name__ == "__main__":
+    import os
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    from btc_b200 import tune as _t
     if len(sys.argv) > 2 and sys.argv[1] == "--sweep":
-        rows = sweep()
+        rows = _t.sweep()
         with open(sys.argv[2], "w") as f:
             json.dump({"graphs": rows}, f, indent=1)
         sys.exit(0)
     if len(sys.argv) > 2 and sys.argv[1] == "--table":
         with open(sys.argv[2]) as f:
-            print(policy_table(json.load(f)["graphs"]))
+            print(_t.policy_table(json.load(f)["graphs"]))
         sys.exit(0)
-    import os
-    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
-    from btc_b200 import tune as _t
     _t.main()

@@ -12,6 +12,7 @@
 // those of bitmap.cu (mark, count, scan, emit, fill), with the graph of an edge found by
 // a binary search over the edge offsets and the graph of a bitmap word by a search over
 // the segment offsets.
+#include <algorithm>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -98,9 +99,20 @@ __global__ void __launch_bounds__(kThreads)
 k_emit_b(const uint32_t* __restrict__ bitmap, uint64_t W, const GraphSeg* __restrict__ segs,
          const uint64_t* __restrict__ bm_off, uint32_t G, const uint32_t* __restrict__ chunk_base,
          uint32_t* __restrict__ prefix, uint32_t* __restrict__ indices,
-         uint32_t* __restrict__ row_indices, uint32_t* __restrict__ indptr)
+         uint32_t* __restrict__ row_indices, uint32_t* __restrict__ indptr,
+         const unsigned long long* __restrict__ tiles, uint32_t cap, uint4* __restrict__ blocks,
+         uint32_t tile_vec4)
 {
     __shared__ uint32_t s_warp[kThreads / kWarp];
+    const unsigned long long T = *tiles;
+    if (T > cap) return;  // more tiles than the arrays hold: nothing is built
+    {
+        // zero this chunk's tiles before k_fill_b ORs bits into them
+        const uint64_t tb = chunk_base[blockIdx.x];
+        const uint64_t te = blockIdx.x + 1 < gridDim.x ? chunk_base[blockIdx.x + 1] : T;
+        for (uint64_t i = tb * tile_vec4 + threadIdx.x; i < te * tile_vec4; i += kThreads)
+            blocks[i] = make_uint4(0u, 0u, 0u, 0u);
+    }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t w0 = (uint64_t)blockIdx.x * kChunk + (uint64_t)threadIdx.x * kWordsPerThread;
     uint32_t x[kWordsPerThread];
@@ -158,8 +170,9 @@ __global__ void __launch_bounds__(kThreads)
 k_fill_b(const int32_t* __restrict__ src, const int32_t* __restrict__ dst, int64_t m,
          const GraphSeg* __restrict__ segs, const int64_t* __restrict__ e_off, uint32_t G,
          const uint32_t* __restrict__ bitmap, const uint32_t* __restrict__ prefix,
-         uint32_t* __restrict__ blocks)
+         uint32_t* __restrict__ blocks, const unsigned long long* __restrict__ tiles, uint32_t cap)
 {
+    if (*tiles > cap) return;  // nothing was emitted
     constexpr int C = 1 << LOG2C;
     constexpr int WPR = C / 32;
     constexpr int TW = 16 * WPR;
@@ -177,9 +190,11 @@ k_fill_b(const int32_t* __restrict__ src, const int32_t* __restrict__ dst, int64
 }
 
 __global__ void k_set_last_b(uint32_t* __restrict__ indptr, uint32_t R,
-                             const unsigned long long* __restrict__ total)
+                             unsigned long long* __restrict__ meta, uint32_t cap)
 {
-    indptr[R] = (uint32_t)*total;
+    const unsigned long long T = meta[kMetaTiles];
+    indptr[R] = (uint32_t)T;
+    meta[kMetaOverflow] = T > cap ? 1ull : 0ull;
 }
 
 }  // namespace bt
@@ -200,6 +215,11 @@ struct btc_batch {
     std::vector<int64_t> h_eoff;
     std::vector<uint64_t> h_bmoff;
     std::vector<uint32_t> h_rowoff;
+    std::vector<int32_t> h_nv;
+    bool built = false;        // the geometry above belongs to a build that succeeded
+    bool pending = false;      // an enqueued rebuild's status is not known yet
+    uint32_t pending_cap = 0;  // the tile capacity that rebuild ran against
+    cudaStream_t pending_stream = nullptr;
     void release()
     {
         g.release_all();
@@ -208,15 +228,118 @@ struct btc_batch {
         bm_off.release();
         row_off.release();
         counts.release();
+        built = pending = false;
     }
 };
+
+// Waits for an enqueued rebuild's metadata and returns its status: BTC_E_RANGE for an
+// out-of-range id, BTC_E_CAPACITY for more tiles than the arrays held (nothing built),
+// BTC_OK (the tile count is then known).
+static int batch_resolve(btc_batch* b)
+{
+    if (!b->pending) return BTC_OK;
+    b->pending = false;
+    btc_bitbsr* g = &b->g;
+    unsigned long long* meta = g->meta.as<unsigned long long>();
+    BTC_CUDA_TRY(cudaMemcpyAsync(g->h_meta, meta, sizeof(unsigned long long) * kMetaSlots,
+                                 cudaMemcpyDeviceToHost, b->pending_stream));
+    BTC_CUDA_TRY(cudaStreamSynchronize(b->pending_stream));
+    if (g->h_meta[kMetaBad] != 0) {
+        b->built = false;
+        return BTC_E_RANGE;
+    }
+    if (g->h_meta[kMetaOverflow] != 0) {
+        b->built = false;
+        return BTC_E_CAPACITY;
+    }
+    g->num_tiles = (uint32_t)g->h_meta[kMetaTiles];
+    return BTC_OK;
+}
+
+// Tiles the batch's arrays hold room for.
+static uint32_t batch_capacity(const btc_batch* b)
+{
+    const btc_bitbsr* g = &b->g;
+    const size_t TW = (size_t)16 * (g->tile_cols / 32);
+    uint64_t c = g->indices.bytes / 4;
+    c = std::min<uint64_t>(c, g->row_indices.bytes / 4);
+    c = std::min<uint64_t>(c, g->blocks.bytes / (4 * TW));
+    c = std::min<uint64_t>(c, g->rowmask.bytes / 4);
+    return (uint32_t)std::min<uint64_t>(c, 0xffffffffull);
+}
+
+// The build after the tile count: emit (indices, row_indices, indptr, cell prefixes, the
+// tiles zeroed), fill, row masks -- all against `cap` tiles, the device tile count deciding
+// (more than cap: nothing is built and the overflow flag is set).
+static int batch_enqueue_tiles(btc_batch* b, const int32_t* d_src, const int32_t* d_dst, int64_t m,
+                               uint32_t cap, cudaStream_t s)
+{
+    btc_bitbsr* g = &b->g;
+    unsigned long long* meta = g->meta.as<unsigned long long>();
+    const uint64_t words = b->h_bmoff[(size_t)b->num_graphs];
+    const size_t chunks = (size_t)((words + bt::kChunk - 1) / bt::kChunk);
+    const GraphSeg* dsegs = b->segs.as<GraphSeg>();
+    const int64_t* deoff = b->e_off.as<int64_t>();
+    const uint32_t G = (uint32_t)b->num_graphs;
+    const uint32_t rows = (uint32_t)g->n_row_blocks;
+    const uint32_t vec4 = 4u * (uint32_t)(g->tile_cols / 32);
+    if (words)
+        bt::k_emit_b<<<(unsigned)chunks, bt::kThreads, 0, s>>>(
+            g->bitmap.as<uint32_t>(), words, dsegs, b->bm_off.as<uint64_t>(), G,
+            g->tile_base.as<uint32_t>(), g->prefix.as<uint32_t>(), g->indices.as<uint32_t>(),
+            g->row_indices.as<uint32_t>(), g->indptr.as<uint32_t>(), meta + kMetaTiles, cap,
+            g->blocks.as<uint4>(), vec4);
+    bt::k_set_last_b<<<1, 1, 0, s>>>(g->indptr.as<uint32_t>(), rows, meta, cap);
+    if (m > 0 && words) {
+        const int egrid = grid_for((m + 3) / 4, bt::kThreads);
+        if (g->tile_cols == 128)
+            bt::k_fill_b<7><<<egrid, bt::kThreads, 0, s>>>(d_src, d_dst, m, dsegs, deoff, G,
+                                                           g->bitmap.as<uint32_t>(), g->prefix.as<uint32_t>(),
+                                                           g->blocks.as<uint32_t>(), meta + kMetaTiles, cap);
+        else
+            bt::k_fill_b<5><<<egrid, bt::kThreads, 0, s>>>(d_src, d_dst, m, dsegs, deoff, G,
+                                                           g->bitmap.as<uint32_t>(), g->prefix.as<uint32_t>(),
+                                                           g->blocks.as<uint32_t>(), meta + kMetaTiles, cap);
+    }
+    BTC_TRY(launch_rowmask(g->tile_cols, g->blocks.as<uint32_t>(), cap, meta + kMetaTiles,
+                           g->indptr.as<uint32_t>(), g->n_row_blocks, g->rowmask.as<uint32_t>(),
+                           meta + kMetaRowMax, s));
+    return cudaGetLastError() == cudaSuccess ? BTC_OK : BTC_E_CUDA;
+}
+
+// Mark and count: the cell bitmap of every graph and the tile count (meta[kMetaTiles]).
+static int batch_enqueue_mark(btc_batch* b, const int32_t* d_src, const int32_t* d_dst, int64_t m,
+                              cudaStream_t s)
+{
+    btc_bitbsr* g = &b->g;
+    unsigned long long* meta = g->meta.as<unsigned long long>();
+    const uint64_t words = b->h_bmoff[(size_t)b->num_graphs];
+    const size_t chunks = (size_t)((words + bt::kChunk - 1) / bt::kChunk);
+    BTC_CUDA_TRY(cudaMemsetAsync(meta, 0, sizeof(unsigned long long) * kMetaSlots, s));
+    if (!words) return BTC_OK;
+    BTC_CUDA_TRY(cudaMemsetAsync(g->bitmap.ptr, 0, sizeof(uint32_t) * words, s));
+    if (m > 0) {
+        const int egrid = grid_for((m + 3) / 4, bt::kThreads);
+        if (g->tile_cols == 128)
+            bt::k_mark_b<7><<<egrid, bt::kThreads, 0, s>>>(d_src, d_dst, m, b->segs.as<GraphSeg>(),
+                                                           b->e_off.as<int64_t>(), (uint32_t)b->num_graphs,
+                                                           g->bitmap.as<uint32_t>(), meta + kMetaBad);
+        else
+            bt::k_mark_b<5><<<egrid, bt::kThreads, 0, s>>>(d_src, d_dst, m, b->segs.as<GraphSeg>(),
+                                                           b->e_off.as<int64_t>(), (uint32_t)b->num_graphs,
+                                                           g->bitmap.as<uint32_t>(), meta + kMetaBad);
+    }
+    BTC_TRY(launch_bitmap_count(g->bitmap.as<uint32_t>(), words, g->tile_base.as<uint32_t>(), s));
+    BTC_TRY(launch_tile_scan(g->tile_base.as<uint32_t>(), (uint32_t)chunks, meta + kMetaTiles, s));
+    return BTC_OK;
+}
 
 static int batch_build_into(btc_batch* b, const int32_t* src, const int32_t* dst,
                             const int64_t* edge_offsets, const int32_t* num_vertices, int32_t G,
                             int tile_cols, uint32_t flags, cudaStream_t s)
 {
     if (G < 1 || !edge_offsets || !num_vertices) return BTC_E_INVAL;
-    if (flags & ~BTC_INPUT_ON_HOST) return BTC_E_INVAL;
+    if (flags & ~(BTC_INPUT_ON_HOST | BTC_BUILD_ASYNC)) return BTC_E_INVAL;
     const int64_t m = edge_offsets[G];
     if (edge_offsets[0] != 0 || m < 0 || (uint64_t)m > (1ull << 32) - (uint64_t)kSortTile)
         return BTC_E_INVAL;
@@ -226,6 +349,28 @@ static int batch_build_into(btc_batch* b, const int32_t* src, const int32_t* dst
         if (num_vertices[i] < 0 || edge_offsets[i + 1] < edge_offsets[i]) return BTC_E_INVAL;
         n_sum += num_vertices[i];
     }
+    btc_bitbsr* g = &b->g;
+
+    // ---- an enqueued rebuild: same graphs' sizes, device input, room for the tiles ------
+    // (no host work, no allocation, no wait: the tile count stays on the device)
+    // (a previous enqueued rebuild still pending is superseded: its status is not kept)
+    const bool same_geometry =
+        b->built && G == b->num_graphs &&
+        (tile_cols == 0 || tile_cols == g->tile_cols) &&
+        std::equal(edge_offsets, edge_offsets + G + 1, b->h_eoff.begin()) &&
+        std::equal(num_vertices, num_vertices + G, b->h_nv.begin());
+    if ((flags & BTC_BUILD_ASYNC) && !(flags & BTC_INPUT_ON_HOST) && same_geometry) {
+        const uint32_t cap = batch_capacity(b);
+        BTC_TRY(batch_enqueue_mark(b, src, dst, m, s));
+        BTC_TRY(batch_enqueue_tiles(b, src, dst, m, cap, s));
+        b->pending = true;
+        b->pending_cap = cap;
+        b->pending_stream = s;
+        return BTC_OK;
+    }
+    if (b->pending) batch_resolve(b);  // an enqueued build still owns the buffers
+    b->built = false;
+
     if (tile_cols == 0) {
         // the engine's tile policy over the whole batch (policy.cu), each sampled edge's
         // locality measured against its own graph's size
@@ -255,6 +400,7 @@ static int batch_build_into(btc_batch* b, const int32_t* src, const int32_t* dst
     b->num_graphs = G;
     b->h_segs.resize((size_t)G);
     b->h_eoff.assign(edge_offsets, edge_offsets + G + 1);
+    b->h_nv.assign(num_vertices, num_vertices + G);
     b->h_bmoff.resize((size_t)G + 1);
     b->h_rowoff.resize((size_t)G + 1);
     uint64_t rows = 0, words = 0;
@@ -280,7 +426,6 @@ static int batch_build_into(btc_batch* b, const int32_t* src, const int32_t* dst
     b->h_bmoff[(size_t)G] = words;
     if (words * 8 > (4ull << 30)) return BTC_E_INVAL;  // bitmap + prefix budget
 
-    btc_bitbsr* g = &b->g;
     BTC_CUDA_TRY(cudaGetDevice(&g->device));
     g->tile_cols = tile_cols;
     g->n = (int32_t)(rows * 16);
@@ -297,7 +442,6 @@ static int batch_build_into(btc_batch* b, const int32_t* src, const int32_t* dst
     }
     BTC_TRY(g->meta.reserve(sizeof(unsigned long long) * kMetaSlots));
     unsigned long long* meta = g->meta.as<unsigned long long>();
-    BTC_CUDA_TRY(cudaMemsetAsync(meta, 0, sizeof(unsigned long long) * kMetaSlots, s));
 
     BTC_TRY(b->segs.reserve(sizeof(GraphSeg) * (size_t)G));
     BTC_TRY(b->e_off.reserve(sizeof(int64_t) * ((size_t)G + 1)));
@@ -326,32 +470,13 @@ static int batch_build_into(btc_batch* b, const int32_t* src, const int32_t* dst
         d_dst = g->in_dst.as<int32_t>();
     }
 
-    // ---- mark, count, scan ----------------------------------------------------------
+    // ---- mark, count, scan; the tile count to size the arrays ----------------------
     const size_t chunks = (size_t)((words + bt::kChunk - 1) / bt::kChunk);
     BTC_TRY(g->bitmap.reserve(sizeof(uint32_t) * (words ? words : 1)));
     BTC_TRY(g->prefix.reserve(sizeof(uint32_t) * (words ? words : 1)));
     BTC_TRY(g->tile_base.reserve(sizeof(uint32_t) * (chunks + 1)));
-    const GraphSeg* dsegs = b->segs.as<GraphSeg>();
-    const int64_t* deoff = b->e_off.as<int64_t>();
-    const int egrid = grid_for((m + 3) / 4, bt::kThreads);
-    if (words) {
-        BTC_CUDA_TRY(cudaMemsetAsync(g->bitmap.ptr, 0, sizeof(uint32_t) * words, s));
-        if (m > 0) {
-            if (tile_cols == 128)
-                bt::k_mark_b<7><<<egrid, bt::kThreads, 0, s>>>(d_src, d_dst, m, dsegs, deoff,
-                                                               (uint32_t)G, g->bitmap.as<uint32_t>(),
-                                                               meta + kMetaBad);
-            else
-                bt::k_mark_b<5><<<egrid, bt::kThreads, 0, s>>>(d_src, d_dst, m, dsegs, deoff,
-                                                               (uint32_t)G, g->bitmap.as<uint32_t>(),
-                                                               meta + kMetaBad);
-        }
-        BTC_TRY(launch_bitmap_count(g->bitmap.as<uint32_t>(), words, g->tile_base.as<uint32_t>(), s));
-        BTC_TRY(launch_tile_scan(g->tile_base.as<uint32_t>(), (uint32_t)chunks, meta + kMetaTiles, s));
-    } else if (m > 0) {
-        // only empty graphs: every edge has an out-of-range id
-        return BTC_E_RANGE;
-    }
+    BTC_TRY(batch_enqueue_mark(b, d_src, d_dst, m, s));
+    if (!words && m > 0) return BTC_E_RANGE;  // only empty graphs: every edge is out of range
     BTC_CUDA_TRY(cudaMemcpyAsync(g->h_meta, meta, sizeof(unsigned long long) * 3,
                                  cudaMemcpyDeviceToHost, s));
     BTC_CUDA_TRY(cudaStreamSynchronize(s));
@@ -366,32 +491,12 @@ static int batch_build_into(btc_batch* b, const int32_t* src, const int32_t* dst
     BTC_TRY(g->indices.reserve(sizeof(uint32_t) * (tiles ? tiles : 1)));
     BTC_TRY(g->row_indices.reserve(sizeof(uint32_t) * (tiles ? tiles : 1)));
     BTC_TRY(g->blocks.reserve(sizeof(uint32_t) * TW * (tiles ? tiles : 1)));
+    BTC_TRY(g->rowmask.reserve(sizeof(uint32_t) * (tiles ? tiles : 1)));
     BTC_TRY(ensure_count_scratch(g));
     BTC_TRY(b->counts.reserve(sizeof(unsigned long long) * (size_t)G));
-    if (tiles) BTC_CUDA_TRY(cudaMemsetAsync(g->blocks.ptr, 0, sizeof(uint32_t) * TW * tiles, s));
-    if (words)
-        bt::k_emit_b<<<(unsigned)chunks, bt::kThreads, 0, s>>>(
-            g->bitmap.as<uint32_t>(), words, dsegs, b->bm_off.as<uint64_t>(), (uint32_t)G,
-            g->tile_base.as<uint32_t>(), g->prefix.as<uint32_t>(), g->indices.as<uint32_t>(),
-            g->row_indices.as<uint32_t>(), g->indptr.as<uint32_t>());
-    bt::k_set_last_b<<<1, 1, 0, s>>>(g->indptr.as<uint32_t>(), (uint32_t)rows, meta + kMetaTiles);
-    if (m > 0 && words) {
-        if (tile_cols == 128)
-            bt::k_fill_b<7><<<egrid, bt::kThreads, 0, s>>>(d_src, d_dst, m, dsegs, deoff, (uint32_t)G,
-                                                           g->bitmap.as<uint32_t>(),
-                                                           g->prefix.as<uint32_t>(),
-                                                           g->blocks.as<uint32_t>());
-        else
-            bt::k_fill_b<5><<<egrid, bt::kThreads, 0, s>>>(d_src, d_dst, m, dsegs, deoff, (uint32_t)G,
-                                                           g->bitmap.as<uint32_t>(),
-                                                           g->prefix.as<uint32_t>(),
-                                                           g->blocks.as<uint32_t>());
-    }
-    BTC_TRY(g->rowmask.reserve(sizeof(uint32_t) * (tiles ? tiles : 1)));
-    BTC_TRY(launch_rowmask(tile_cols, g->blocks.as<uint32_t>(), g->num_tiles, nullptr,
-                           g->indptr.as<uint32_t>(), g->n_row_blocks, g->rowmask.as<uint32_t>(),
-                           meta + kMetaRowMax, s));
-    return cudaGetLastError() == cudaSuccess ? BTC_OK : BTC_E_CUDA;
+    BTC_TRY(batch_enqueue_tiles(b, d_src, d_dst, m, (uint32_t)tiles, s));
+    b->built = true;
+    return BTC_OK;
 }
 
 namespace btc200 {
@@ -440,27 +545,35 @@ int btc_batch_count(btc_batch* b, int tau, btc_stream_t stream, unsigned long lo
     if (tau == BTC_TAU_DEFAULT) tau = default_tau(g->tile_cols);
     if (tau < 0) return BTC_E_INVAL;
     BTC_TRY(ensure_count_scratch(g));
+    if (!b->built && !b->pending) return BTC_E_INVAL;  // the last build failed
     unsigned long long* counts = d_counts ? d_counts : b->counts.as<unsigned long long>();
     const size_t bytes = sizeof(unsigned long long) * (size_t)b->num_graphs;
     BTC_CUDA_TRY(cudaMemsetAsync(counts, 0, bytes, stream));
     CountScratch scr{g->partials.as<unsigned long long>(), g->done.as<unsigned int>(),
                      reinterpret_cast<unsigned long long*>(g->done.as<char>() + 8),
                      g->result.as<unsigned long long>(), nullptr};
+    // after an enqueued rebuild the kernel reads the tile count (and the build's status)
+    // from the device, within the capacity; the schedule follows the previous count
+    const unsigned long long* build_meta = b->pending ? g->meta.as<unsigned long long>() : nullptr;
     BTC_TRY(launch_count(g->tile_cols, g->indptr.as<uint32_t>(), g->indices.as<uint32_t>(),
-                         g->row_indices.as<uint32_t>(), g->blocks.as<uint32_t>(), g->num_tiles,
-                         g->n_row_blocks, tau, scr, stream, b->row_off.as<uint32_t>(),
-                         (uint32_t)b->num_graphs, counts, g->rowmask.as<uint32_t>(), nullptr,
-                         0, g->meta.as<unsigned long long>() + kMetaRowMax));
+                         g->row_indices.as<uint32_t>(), g->blocks.as<uint32_t>(),
+                         b->pending ? b->pending_cap : g->num_tiles, g->n_row_blocks, tau, scr,
+                         stream, b->row_off.as<uint32_t>(), (uint32_t)b->num_graphs, counts,
+                         g->rowmask.as<uint32_t>(), nullptr, 0,
+                         g->meta.as<unsigned long long>() + kMetaRowMax, 0, 0xffffffffu, build_meta,
+                         g->num_tiles));
     if (h_counts) {
         BTC_CUDA_TRY(cudaMemcpyAsync(h_counts, counts, bytes, cudaMemcpyDeviceToHost, stream));
         BTC_CUDA_TRY(cudaStreamSynchronize(stream));
+        return batch_resolve(b);  // an enqueued rebuild's failure shows here
     }
     return BTC_OK;
 }
 
-int btc_batch_info(const btc_batch* b, btc_bitbsr_view* v)
+int btc_batch_info(btc_batch* b, btc_bitbsr_view* v)
 {
     if (!b) return BTC_E_INVAL;
+    BTC_TRY(batch_resolve(b));
     return btc_bitbsr_info(&b->g, v);
 }
 

@@ -14,7 +14,9 @@
 //                row_indices of each set cell, indptr at row-block starts; each CTA
 //                zeroes its chunk's tiles, the last one writes indptr[R]
 //   k_fill_bm    second pass over the edges: tile = prefix[word] + popc(lower bits of
-//                the word); OR the edge's bit into the tile
+//                the word); OR the edge's bit into the tile; where the count wants row
+//                masks (8 or more tiles per row block), the edge whose OR finds its tile
+//                word empty also sets its row's bit in the tile's row mask
 //
 // Two reads of the edge list, one read and one write of the bitmap and its prefix
 // array, one write of the tiles: no sort.  Duplicate edges OR the same bit.
@@ -207,7 +209,8 @@ k_bm_emit(const uint32_t* __restrict__ bitmap, uint64_t W, uint64_t wpr,
           const uint32_t* __restrict__ chunk_base, uint2* __restrict__ cellpp,
           uint32_t* __restrict__ indices, uint32_t* __restrict__ row_indices,
           uint32_t* __restrict__ indptr, unsigned long long* meta, uint32_t cap,
-          unsigned long long* host_meta, int32_t R, uint4* __restrict__ blocks, uint32_t tile_vec4)
+          unsigned long long* host_meta, int32_t R, uint4* __restrict__ blocks, uint32_t tile_vec4,
+          uint32_t* __restrict__ rowmask)
 {
     __shared__ uint32_t s_warp[kThreads / kWarp];
     const unsigned long long T = meta[kMetaTiles];
@@ -219,6 +222,9 @@ k_bm_emit(const uint32_t* __restrict__ bitmap, uint64_t W, uint64_t wpr,
         const uint64_t te = blockIdx.x + 1 < gridDim.x ? chunk_base[blockIdx.x + 1] : T;
         for (uint64_t i = tb * tile_vec4 + threadIdx.x; i < te * tile_vec4; i += kThreads)
             blocks[i] = make_uint4(0u, 0u, 0u, 0u);
+        // and their row-occupancy masks, which k_fill_bm sets
+        if (rowmask)
+            for (uint64_t i = tb + threadIdx.x; i < te; i += kThreads) rowmask[i] = 0u;
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t w0 = (uint64_t)blockIdx.x * (kThreads * WPT) + (uint64_t)threadIdx.x * WPT;
@@ -282,9 +288,14 @@ __global__ void __launch_bounds__(kThreads)
 k_fill_bm(const int32_t* __restrict__ src, const int32_t* __restrict__ dst, int64_t m, int32_t n,
           const int32_t* __restrict__ rank, uint64_t wpr, const uint32_t* __restrict__ bitmap,
           const uint2* __restrict__ cellpp, uint32_t* __restrict__ blocks,
-          const unsigned long long* __restrict__ d_tiles, uint32_t cap)
+          const unsigned long long* __restrict__ d_tiles, uint32_t cap, uint32_t* __restrict__ rowmask,
+          int32_t R)
 {
-    if (*d_tiles > cap) return;  // overflowed tile arrays: the builder redoes this step
+    const unsigned long long T = *d_tiles;
+    if (T > cap) return;  // overflowed tile arrays: the builder redoes this step
+    // row-occupancy masks: wanted when row blocks average 8 or more tiles (the row-wise
+    // count's condition, on the device tile count)
+    if (T < 8ull * (unsigned long long)(R > 0 ? R : 0)) rowmask = nullptr;
     constexpr int C = 1 << LOG2C;
     constexpr int WPR = C / 32;
     constexpr int TW = 16 * WPR;
@@ -320,7 +331,14 @@ k_fill_bm(const int32_t* __restrict__ src, const int32_t* __restrict__ dst, int6
             const uint32_t below = (1u << ((c[k] >> LOG2C) & 31u)) - 1u;
             const uint32_t t = pre[k] + __popc(word[k] & below);
             const uint32_t cl = c[k] & (C - 1);
-            atomicOr(&blocks[(size_t)t * TW + (r[k] & 15u) * WPR + (cl >> 5)], 1u << (cl & 31u));
+            uint32_t* tw = &blocks[(size_t)t * TW + (r[k] & 15u) * WPR + (cl >> 5)];
+            if (rowmask) {
+                // the edge that finds its tile word empty marks the row: one mask atomic
+                // per non-empty word, none per edge of a busy row
+                if (atomicOr(tw, 1u << (cl & 31u)) == 0u) atomicOr(&rowmask[t], 1u << (r[k] & 15u));
+            } else {
+                atomicOr(tw, 1u << (cl & 31u));
+            }
         }
     }
 }
@@ -422,7 +440,8 @@ int bitmap_emit_and_fill(const BuildGeom& g, const int32_t* src, const int32_t* 
                          const int32_t* rank, const uint32_t* bitmap, const uint32_t* chunk_base,
                          uint2* cellpp, uint32_t* indices, uint32_t* row_indices,
                          uint32_t* indptr, uint32_t* blocks, unsigned long long* meta,
-                         uint32_t cap, unsigned long long* host_meta, cudaStream_t s)
+                         uint32_t cap, unsigned long long* host_meta, cudaStream_t s,
+                         uint32_t* rowmask)
 {
     const unsigned long long* meta_tiles = meta + kMetaTiles;
     const uint64_t wpr = bitmap_words_per_row(g);
@@ -435,7 +454,7 @@ int bitmap_emit_and_fill(const BuildGeom& g, const int32_t* src, const int32_t* 
 #define BTC_EMIT(WPT)                                                                         \
     bm::k_bm_emit<WPT><<<grid, bm::kThreads, 0, s>>>(bitmap, W, wpr, chunk_base, cellpp, indices, \
                                                     row_indices, indptr, meta, cap, host_meta, R, \
-                                                    b4, vec4)
+                                                    b4, vec4, rowmask)
         switch (bitmap_wpt(W)) {
         case 16: BTC_EMIT(16); break;
         case 4: BTC_EMIT(4); break;
@@ -448,10 +467,12 @@ int bitmap_emit_and_fill(const BuildGeom& g, const int32_t* src, const int32_t* 
     if (m > 0 && W > 0) {
         if (g.tile_cols == 128)
             bm::k_fill_bm<7><<<edge_grid(m), bm::kThreads, 0, s>>>(
-                src, dst, m, g.n, rank, wpr, bitmap, cellpp, blocks, meta_tiles, cap);
+                src, dst, m, g.n, rank, wpr, bitmap, cellpp, blocks, meta_tiles, cap, rowmask,
+                g.n_row_blocks);
         else
             bm::k_fill_bm<5><<<edge_grid(m), bm::kThreads, 0, s>>>(
-                src, dst, m, g.n, rank, wpr, bitmap, cellpp, blocks, meta_tiles, cap);
+                src, dst, m, g.n, rank, wpr, bitmap, cellpp, blocks, meta_tiles, cap, rowmask,
+                g.n_row_blocks);
     }
     return cudaGetLastError() == cudaSuccess ? BTC_OK : BTC_E_CUDA;
 }
@@ -490,7 +511,8 @@ template <int WPR>
 __global__ void k_rowmask(const uint32_t* __restrict__ blocks, uint32_t cap,
                           const unsigned long long* __restrict__ d_tiles,
                           const uint32_t* __restrict__ indptr, uint32_t R,
-                          uint32_t* __restrict__ rowmask, unsigned long long* __restrict__ row_max)
+                          uint32_t* __restrict__ rowmask, unsigned long long* __restrict__ row_max,
+                          bool masks)
 {
     const unsigned long long T = d_tiles ? *d_tiles : cap;
     if (T > cap) return;  // overflowed tile arrays: the builder redoes this step
@@ -504,7 +526,7 @@ __global__ void k_rowmask(const uint32_t* __restrict__ blocks, uint32_t cap,
     if ((threadIdx.x & 31) == 0 && mx) atomicMax(row_max, (unsigned long long)mx);
     // the masks serve only the heavy count variant, which reads them only when row
     // blocks average 8 or more tiles (the same test on the same count)
-    if ((uint64_t)num_tiles < 8ull * (uint64_t)R) return;
+    if (!masks || (uint64_t)num_tiles < 8ull * (uint64_t)R) return;
 
     for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < num_tiles;
          t += (uint64_t)gridDim.x * blockDim.x) {
@@ -533,15 +555,15 @@ __global__ void k_rowmask(const uint32_t* __restrict__ blocks, uint32_t cap,
 
 int launch_rowmask(int tile_cols, const uint32_t* blocks, uint32_t cap,
                    const unsigned long long* d_tiles, const uint32_t* indptr, int32_t n_row_blocks,
-                   uint32_t* rowmask, unsigned long long* row_max, cudaStream_t s)
+                   uint32_t* rowmask, unsigned long long* row_max, cudaStream_t s, bool masks)
 {
     const uint32_t R = n_row_blocks > 0 ? (uint32_t)n_row_blocks : 0u;
     if (cap || R) {
-        const int grid = grid_for((int64_t)max(cap, R), 256);
+        const int grid = grid_for((int64_t)(masks ? max(cap, R) : R), 256);
         if (tile_cols == 128)
-            bm::k_rowmask<4><<<grid, 256, 0, s>>>(blocks, cap, d_tiles, indptr, R, rowmask, row_max);
+            bm::k_rowmask<4><<<grid, 256, 0, s>>>(blocks, cap, d_tiles, indptr, R, rowmask, row_max, masks);
         else
-            bm::k_rowmask<1><<<grid, 256, 0, s>>>(blocks, cap, d_tiles, indptr, R, rowmask, row_max);
+            bm::k_rowmask<1><<<grid, 256, 0, s>>>(blocks, cap, d_tiles, indptr, R, rowmask, row_max, masks);
     }
     return cudaGetLastError() == cudaSuccess ? BTC_OK : BTC_E_CUDA;
 }

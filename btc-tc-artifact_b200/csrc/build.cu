@@ -45,16 +45,50 @@ __device__ __forceinline__ uint32_t warp_sum(uint32_t v)
 // ---------------------------------------------------------------------------
 // degree relabel
 // ---------------------------------------------------------------------------
-__global__ void k_degree(const int32_t* __restrict__ src, const int32_t* __restrict__ dst,
-                         int64_t m, int32_t n, uint32_t* __restrict__ deg)
+// Degree count.  On power-law inputs a few hub vertices take a large share of the
+// increments, and atomics on one global word serialise; so each CTA keeps a small table
+// of counters in shared memory: a vertex takes the free slot its hash points to the first
+// time the CTA sees it (compare-and-swap), later increments of it stay in shared memory,
+// and the table is added to the global counters once when the CTA ends.  Hubs appear
+// often and early, so they own slots in every CTA; a vertex whose slot is taken by
+// another counts in global memory as before.
+constexpr int kDegSlots = 2048;
+constexpr uint32_t kDegFree = 0xffffffffu;
+
+__device__ __forceinline__ void degree_add(uint32_t v, uint32_t* __restrict__ keys,
+                                           uint32_t* __restrict__ cnt, uint32_t* __restrict__ deg)
 {
+    const uint32_t slot = (v * 0x9E3779B1u) >> (32 - 11);  // kDegSlots = 2^11
+    uint32_t k = keys[slot];
+    if (k == kDegFree) {
+        const uint32_t prev = atomicCAS(&keys[slot], kDegFree, v);
+        k = prev == kDegFree ? v : prev;
+    }
+    if (k == v) atomicAdd(&cnt[slot], 1u);
+    else atomicAdd(&deg[v], 1u);
+}
+
+__global__ void __launch_bounds__(256)
+k_degree(const int32_t* __restrict__ src, const int32_t* __restrict__ dst,
+         int64_t m, int32_t n, uint32_t* __restrict__ deg)
+{
+    static_assert(kDegSlots == 1 << 11, "degree_add hashes to 11 bits");
+    __shared__ uint32_t keys[kDegSlots], cnt[kDegSlots];
+    for (int i = threadIdx.x; i < kDegSlots; i += blockDim.x) {
+        keys[i] = kDegFree;
+        cnt[i] = 0;
+    }
+    __syncthreads();
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
          i += (int64_t)gridDim.x * blockDim.x) {
         const int32_t u = src[i], v = dst[i];
         if (u == v || u < 0 || v < 0 || u >= n || v >= n) continue;
-        atomicAdd(&deg[u], 1u);
-        atomicAdd(&deg[v], 1u);
+        degree_add((uint32_t)u, keys, cnt, deg);
+        degree_add((uint32_t)v, keys, cnt, deg);
     }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kDegSlots; i += blockDim.x)
+        if (keys[i] != kDegFree && cnt[i]) atomicAdd(&deg[keys[i]], cnt[i]);
 }
 
 // key = ((dmax - deg) << 32) | v ; sorted ascending on bits [32, 32+db) with a stable

@@ -30,7 +30,7 @@ int bitmap_mark_and_count(const BuildGeom&, const int32_t*, const int32_t*, int6
 int bitmap_emit_and_fill(const BuildGeom&, const int32_t*, const int32_t*, int64_t, const int32_t*,
                          const uint32_t*, const uint32_t*, uint2*, uint32_t*, uint32_t*, uint32_t*,
                          uint32_t*, unsigned long long*, uint32_t, unsigned long long*,
-                         cudaStream_t);
+                         cudaStream_t, uint32_t*);
 int launch_popcount_sum(int, const uint32_t*, uint64_t, unsigned long long*, cudaStream_t);
 int launch_indptr(const uint32_t*, uint32_t, int32_t, uint32_t*, cudaStream_t);
 int launch_density(int, const uint32_t*, uint32_t, unsigned long long*, cudaStream_t);
@@ -188,10 +188,12 @@ static int enqueue_build(btc_bitbsr* g, const BuildPlan& P, uint64_t** sorted_ou
                                          g->bitmap.as<uint32_t>(), g->tile_base.as<uint32_t>(),
                                          g->prefix.as<uint2>(), g->indices.as<uint32_t>(),
                                          g->row_indices.as<uint32_t>(), g->indptr.as<uint32_t>(),
-                                         g->blocks.as<uint32_t>(), meta, P.cap, g->d_hmeta, s));
+                                         g->blocks.as<uint32_t>(), meta, P.cap, g->d_hmeta, s,
+                                         g->rowmask.as<uint32_t>()));
+            // the fill pass set the row masks; this pass finds the longest row-block list
             BTC_TRY(launch_rowmask(geom.tile_cols, g->blocks.as<uint32_t>(), P.cap,
                                    meta + kMetaTiles, g->indptr.as<uint32_t>(), geom.n_row_blocks,
-                                   g->rowmask.as<uint32_t>(), meta + kMetaRowMax, s));
+                                   g->rowmask.as<uint32_t>(), meta + kMetaRowMax, s, false));
             if (P.row_index) BTC_TRY(enqueue_row_index(g, meta + kMetaTiles, P.cap, s));
         }
     } else {
@@ -405,12 +407,14 @@ static int build_into(btc_bitbsr* g, const int32_t* src, const int32_t* dst, int
     BTC_TRY(g->indices.reserve(sizeof(uint32_t) * (tiles ? tiles : 1)));
     BTC_TRY(g->row_indices.reserve(sizeof(uint32_t) * (tiles ? tiles : 1)));
     BTC_TRY(g->blocks.reserve(sizeof(uint32_t) * TW * (tiles ? tiles : 1)));
+    BTC_TRY(g->rowmask.reserve(sizeof(uint32_t) * (tiles ? tiles : 1)));
     if (P.use_bitmap) {
         BTC_TRY(bitmap_emit_and_fill(geom, P.d_src, P.d_dst, m, P.degree ? g->rank.as<int32_t>() : nullptr,
                                      g->bitmap.as<uint32_t>(), g->tile_base.as<uint32_t>(),
                                      g->prefix.as<uint2>(), g->indices.as<uint32_t>(),
                                      g->row_indices.as<uint32_t>(), g->indptr.as<uint32_t>(),
-                                     g->blocks.as<uint32_t>(), meta, (uint32_t)tiles, nullptr, s));
+                                     g->blocks.as<uint32_t>(), meta, (uint32_t)tiles, nullptr, s,
+                                     g->rowmask.as<uint32_t>()));
     } else {
         if (tiles)
             BTC_CUDA_TRY(cudaMemsetAsync(g->blocks.ptr, 0, sizeof(uint32_t) * TW * tiles, s));
@@ -420,10 +424,10 @@ static int build_into(btc_bitbsr* g, const int32_t* src, const int32_t* dst, int
         BTC_TRY(launch_indptr(g->row_indices.as<uint32_t>(), g->num_tiles, geom.n_row_blocks,
                               g->indptr.as<uint32_t>(), s));
     }
-    BTC_TRY(g->rowmask.reserve(sizeof(uint32_t) * (tiles ? tiles : 1)));
+    // the bitmap path's fill pass set the row masks; the radix path's are computed here
     BTC_TRY(launch_rowmask(tile_cols, g->blocks.as<uint32_t>(), g->num_tiles, nullptr,
                            g->indptr.as<uint32_t>(), g->n_row_blocks, g->rowmask.as<uint32_t>(),
-                           meta + kMetaRowMax, s));
+                           meta + kMetaRowMax, s, !P.use_bitmap));
     if (P.row_index) BTC_TRY(enqueue_row_index(g, nullptr, g->num_tiles, s));
     return BTC_OK;
 }

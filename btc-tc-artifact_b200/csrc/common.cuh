@@ -165,9 +165,10 @@ int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
 // *row_max = max(*row_max, the most tiles in one row block), which picks the count
 // kernel's schedule (the caller zeroes it).  Runs after the tiles are filled.  Writes
 // nothing when T > cap (the tile arrays overflowed).
+// masks = false: only *row_max (the bitmap builder's fill pass sets the masks itself).
 int launch_rowmask(int tile_cols, const uint32_t* blocks, uint32_t cap,
                    const unsigned long long* d_tiles, const uint32_t* indptr, int32_t n_row_blocks,
-                   uint32_t* rowmask, unsigned long long* row_max, cudaStream_t s);
+                   uint32_t* rowmask, unsigned long long* row_max, cudaStream_t s, bool masks = true);
 
 // Row index of the row-wise count kernel (rowindex.cu): for vertex u, ent[off[u],
 // off[u+1]) lists (column block, tile) of the tiles whose row u % 16 holds a bit, in tile

@@ -15,8 +15,11 @@
 // nothing for it, and degree order keeps its hub rows short) once it reaches the front
 // of the queue; a batch being formed passes over such requests and takes the small ones
 // behind them.  Solo rebuilds are enqueued without a host wait, so the engine thread
-// keeps filling the other slots meanwhile.  With slots = 1 and max_batch_graphs = 1 the
-// same server is the plain one-request-at-a-time path.
+// keeps filling the other slots meanwhile.  All slots share one solo handle, one solo
+// launch at a time: the handle's buffers grow to the largest request once, instead of
+// once per slot (a growth frees and allocates device memory, which waits for every
+// stream, the other slots' batches included).  With slots = 1 and max_batch_graphs = 1
+// the same server is the plain one-request-at-a-time path.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -80,15 +83,13 @@ struct Slot {
     cudaEvent_t start = nullptr;  // recorded before the slot's first copy
     cudaEvent_t done = nullptr;
     btc_batch* batch = nullptr;
-    btc_bitbsr* solo = nullptr;  // large requests: one graph, descending-degree order
     btc200::DevBuf d_counts, d_src, d_dst;
     PinnedBuf h_src, h_dst, h_counts;
     std::vector<Request> reqs;
     std::vector<int64_t> offsets;
     std::vector<int32_t> nv;
-    size_t device_bytes = 0;
+    size_t device_bytes = 0;  // batch handle and edge copies
     bool busy = false;
-    bool solo_async = false;  // the solo handle's rebuild was enqueued without a wait
     bool solo_launch = false; // the slot's current launch runs one request alone
 };
 
@@ -103,6 +104,10 @@ struct btc_server {
     std::deque<Request> pending;
     std::vector<btc_server_result> done;
     std::vector<Slot> slots;
+    // large requests: one graph, descending-degree order, on whichever slot runs it
+    btc_bitbsr* solo = nullptr;
+    int solo_slot = -1;        // the slot whose launch holds the solo handle, or -1
+    bool solo_async = false;   // its rebuild was enqueued without a wait
     std::thread engine;
     bool stop = false;
     uint64_t next_id = 1;
@@ -121,7 +126,7 @@ namespace {
 
 size_t slot_budget_in_use(btc_server* s, const Slot* except)
 {
-    size_t b = 0;
+    size_t b = s->solo ? s->solo->device_bytes() : 0;
     for (const Slot& sl : s->slots)
         if (&sl != except) b += sl.device_bytes;
     return b;
@@ -164,6 +169,7 @@ void publish(btc_server* s, Slot& sl, int status)
     for (const Request& q : sl.reqs) s->stats.edges += (uint64_t)q.m;
     sl.reqs.clear();
     sl.busy = false;
+    if (s->solo_slot == (int)(&sl - s->slots.data())) s->solo_slot = -1;
     s->cv.notify_all();
 }
 
@@ -233,16 +239,18 @@ int launch_slot(btc_server* s, Slot& sl)
         // its hub rows short (the engine's tile policy then picks 16x128)
         // Rebuilds are enqueued without a host wait (BTC_BUILD_ASYNC), so the engine
         // thread goes on filling the other slots; finish_solo checks the build's status.
-        if (!sl.solo) {
+        // The admission loop handed this slot the solo handle (s->solo_slot); the slot
+        // that used it before has been published, so its stream is done with it.
+        if (!s->solo) {
             st = btc_build_bitbsr(ds, dd, m, sl.reqs[0].n, 0, BTC_ORIENT_DEGREE, sl.stream,
-                                  &sl.solo);
+                                  &s->solo);
         } else {
-            st = btc_rebuild_bitbsr(sl.solo, ds, dd, m, sl.reqs[0].n, 0,
+            st = btc_rebuild_bitbsr(s->solo, ds, dd, m, sl.reqs[0].n, 0,
                                     BTC_ORIENT_DEGREE | BTC_BUILD_ASYNC, sl.stream);
-            sl.solo_async = st == BTC_OK;
+            s->solo_async = st == BTC_OK;
         }
         if (st != BTC_OK) return st;
-        st = btc_count_async(sl.solo, s->cfg.tau, sl.stream, sl.d_counts.as<unsigned long long>());
+        st = btc_count_async(s->solo, s->cfg.tau, sl.stream, sl.d_counts.as<unsigned long long>());
         if (st != BTC_OK) return st;
     } else {
         if (!sl.batch)
@@ -258,8 +266,8 @@ int launch_slot(btc_server* s, Slot& sl)
     }
     // device memory held by this slot (read directly: btc_*_info would also count the
     // unique edges, a device pass not needed here)
-    sl.device_bytes = (sl.batch ? btc200::batch_device_bytes(sl.batch) : 0) +
-                      (sl.solo ? sl.solo->device_bytes() : 0) + sl.d_src.bytes + sl.d_dst.bytes;
+    sl.device_bytes = (sl.batch ? btc200::batch_device_bytes(sl.batch) : 0) + sl.d_src.bytes +
+                      sl.d_dst.bytes;
     if (cudaMemcpyAsync(sl.h_counts.p, sl.d_counts.ptr, sizeof(unsigned long long) * (size_t)G,
                         cudaMemcpyDeviceToHost, sl.stream) != cudaSuccess ||
         cudaEventRecord(sl.done, sl.stream) != cudaSuccess)
@@ -273,17 +281,17 @@ int launch_slot(btc_server* s, Slot& sl)
 // Status of a finished slot whose solo graph was rebuilt without a wait: an enqueued
 // build that found more tiles than the handle's arrays hold built nothing, so it is
 // redone here with a waiting rebuild from the slot's device copy of the edges.
-int finish_solo(Slot& sl, int tau)
+int finish_solo(btc_server* s, Slot& sl, int tau)
 {
-    if (!sl.solo_async) return BTC_OK;
-    sl.solo_async = false;
-    int st = resolve_build(sl.solo);
+    if (!sl.solo_launch || !s->solo_async) return BTC_OK;
+    s->solo_async = false;
+    int st = resolve_build(s->solo);
     if (st != BTC_E_CAPACITY) return st;
     const int64_t m = sl.offsets.back();
-    st = btc_rebuild_bitbsr(sl.solo, sl.d_src.as<int32_t>(), sl.d_dst.as<int32_t>(), m,
+    st = btc_rebuild_bitbsr(s->solo, sl.d_src.as<int32_t>(), sl.d_dst.as<int32_t>(), m,
                             sl.reqs[0].n, 0, BTC_ORIENT_DEGREE, sl.stream);
     if (st == BTC_OK)
-        st = btc_count_async(sl.solo, tau, sl.stream, sl.d_counts.as<unsigned long long>());
+        st = btc_count_async(s->solo, tau, sl.stream, sl.d_counts.as<unsigned long long>());
     if (st == BTC_OK &&
         (cudaMemcpyAsync(sl.h_counts.p, sl.d_counts.ptr, sizeof(unsigned long long),
                          cudaMemcpyDeviceToHost, sl.stream) != cudaSuccess ||
@@ -298,7 +306,7 @@ void engine_loop(btc_server* s)
     for (;;) {
         // 1. publish finished slots
         for (Slot& sl : s->slots)
-            if (sl.busy && cudaEventQuery(sl.done) == cudaSuccess) publish(s, sl, finish_solo(sl, s->cfg.tau));
+            if (sl.busy && cudaEventQuery(sl.done) == cudaSuccess) publish(s, sl, finish_solo(s, sl, s->cfg.tau));
 
         // 2. fill a free slot from the queue
         Slot* free_slot = nullptr;
@@ -338,8 +346,8 @@ void engine_loop(btc_server* s)
                        scanned++ < max_scan) {
                     Request& q = *it;
                     const int64_t qm = q.m;
-                    // a large request runs alone (solo path)
-                    if (!sl.reqs.empty() && qm >= s->cfg.solo_edges) {
+                    // a large request runs alone (solo path), when the solo handle is free
+                    if (qm >= s->cfg.solo_edges && (!sl.reqs.empty() || s->solo_slot >= 0)) {
                         ++it;
                         continue;
                     }
@@ -368,7 +376,10 @@ void engine_loop(btc_server* s)
                     sl.offsets.push_back(m);
                     sl.nv.push_back(sl.reqs.back().n);
                     it = s->pending.erase(it);
-                    if (qm >= s->cfg.solo_edges) break;
+                    if (qm >= s->cfg.solo_edges) {
+                        s->solo_slot = (int)(&sl - s->slots.data());
+                        break;
+                    }
                 }
                 if (!rejected.empty()) {
                     s->done.insert(s->done.end(), rejected.begin(), rejected.end());
@@ -528,9 +539,9 @@ void btc_server_destroy(btc_server* s)
         s->cv.notify_all();
     }
     if (s->engine.joinable()) s->engine.join();
+    if (s->solo) btc_free(s->solo);
     for (Slot& sl : s->slots) {
         if (sl.batch) btc_batch_free(sl.batch);
-        if (sl.solo) btc_free(sl.solo);
         sl.d_counts.release();
         sl.d_src.release();
         sl.d_dst.release();

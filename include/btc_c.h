@@ -308,7 +308,17 @@ BTC_API int btc_batch_build(const int32_t* src, const int32_t* dst, const int64_
                             const int32_t* num_vertices, int32_t num_graphs, int tile_cols,
                             uint32_t flags, btc_stream_t stream, btc_batch** out);
 
-/* Rebuilds into an existing batch, reusing its device buffers when large enough. */
+/* Rebuilds into an existing batch, reusing its device buffers when large enough.
+ * With BTC_BUILD_ASYNC in flags, device input and the same graphs' sizes as the batch's
+ * last successful build (num_graphs, edge_offsets, num_vertices, tile width; the edges may
+ * differ), the rebuild is enqueued against the arrays the batch holds without host work,
+ * allocation or a wait, so it can be captured in a CUDA graph together with
+ * btc_batch_count(..., h_counts = NULL); its status comes with the next call that waits
+ * (btc_batch_count with h_counts, btc_batch_info, a waiting rebuild): BTC_E_RANGE for an
+ * out-of-range id, BTC_E_CAPACITY for more tiles than the arrays held (nothing built, the
+ * counts are 0; rebuild without the flag).  Another enqueued rebuild before that call
+ * replaces it (its status is not kept).  Otherwise the flag is ignored and the rebuild
+ * waits once, as btc_batch_build does. */
 BTC_API int btc_batch_rebuild(btc_batch* b, const int32_t* src, const int32_t* dst,
                               const int64_t* edge_offsets, const int32_t* num_vertices,
                               int32_t num_graphs, int tile_cols, uint32_t flags,
@@ -321,7 +331,7 @@ BTC_API int btc_batch_count(btc_batch* b, int tau, btc_stream_t stream,
                             unsigned long long* d_counts, unsigned long long* h_counts);
 
 /* The union graph's Bit-BSR (reference layout) and sizes. */
-BTC_API int btc_batch_info(const btc_batch* b, btc_bitbsr_view* v);
+BTC_API int btc_batch_info(btc_batch* b, btc_bitbsr_view* v);
 
 /* First row block of each graph in the union (num_graphs+1 host entries). */
 BTC_API int btc_batch_row_offsets(const btc_batch* b, uint32_t* row_offsets);

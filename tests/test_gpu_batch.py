@@ -74,3 +74,97 @@ def test_batch_rejects_bad_input():
     assert e.value.status == _lib.BTC_E_RANGE
     with pytest.raises(BtcError):
         Batch([(np.array([0], np.int32), np.array([1], np.int32), 5)], tile_cols=64)
+
+
+def test_enqueued_rebuild_and_cuda_graph():
+    """btc_batch_rebuild with BTC_BUILD_ASYNC (same graphs' sizes, device edges) enqueues
+    the build without a wait, so rebuild + count can be captured in a CUDA graph; replays
+    count whatever edges the buffers hold then."""
+    gs = [golden_graph(nm) for nm in NAMES]
+    want = [load_golden()[nm]["count"] for nm in NAMES]
+    src, dst, off, nv = Batch.concat(gs)
+    d_src, d_dst = torch.from_numpy(src).cuda(), torch.from_numpy(dst).cuda()
+    args = dict(src=d_src, dst=d_dst, offsets=off, num_vertices=nv, tile_cols=32)
+    b = Batch(**args)
+    assert b.count().tolist() == want
+    out = torch.zeros(len(gs), dtype=torch.int64, device="cuda")
+    b.rebuild(**args, asynchronous=True)
+    b.count_async(out.data_ptr())
+    assert out.cpu().tolist() == want
+    assert b.count().tolist() == want  # the waiting call reports the enqueued build's status
+
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        b.rebuild(**args, stream=s, asynchronous=True)
+        b.count_async(out.data_ptr(), stream=s)
+    s.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=s):
+        b.rebuild(**args, stream=s, asynchronous=True)
+        b.count_async(out.data_ptr(), stream=s)
+    for _ in range(3):
+        out.zero_()
+        graph.replay()
+        torch.cuda.synchronize()
+        assert out.cpu().tolist() == want
+    # other edges in the same buffers (src and dst swapped: the same undirected graphs in
+    # another orientation); the replay builds from what the buffers hold now
+    tmp = d_src.clone()
+    d_src.copy_(d_dst)
+    d_dst.copy_(tmp)
+    out.zero_()
+    graph.replay()
+    torch.cuda.synchronize()
+    assert out.cpu().tolist() == want
+    b.free()
+
+
+def test_enqueued_rebuild_failures_surface_at_the_next_wait():
+    gs = [golden_graph("K33"), golden_graph("stencil27_4")]
+    src, dst, off, nv = Batch.concat(gs)
+    d_src, d_dst = torch.from_numpy(src).cuda(), torch.from_numpy(dst).cuda()
+    b = Batch(src=d_src, dst=d_dst, offsets=off, num_vertices=nv, tile_cols=128)
+    want = b.count().tolist()
+    # an out-of-range id: nothing counted, BTC_E_RANGE at the waiting count
+    bad = d_src.clone()
+    bad[3] = 1 << 20
+    b.rebuild(src=bad, dst=d_dst, offsets=off, num_vertices=nv, tile_cols=128, asynchronous=True)
+    with pytest.raises(BtcError) as e:
+        b.count()
+    assert e.value.status == _lib.BTC_E_RANGE
+    # the batch refuses to count until a rebuild succeeds
+    with pytest.raises(BtcError):
+        b.count()
+    b.rebuild(src=d_src, dst=d_dst, offsets=off, num_vertices=nv, tile_cols=128)
+    assert b.count().tolist() == want
+    b.free()
+
+
+def test_enqueued_rebuild_needing_more_tiles_reports_capacity():
+    """A batch first built with graph 1's edges all on one vertex pair holds arrays for a
+    few tiles; an enqueued rebuild with the real edges (the same sizes) needs more: it
+    builds nothing and reports BTC_E_CAPACITY at the next wait; a waiting rebuild grows
+    the arrays."""
+    gs = [golden_graph("K33"), golden_graph("stencil27_10")]
+    want = [load_golden()[nm]["count"] for nm in ("K33", "stencil27_10")]
+    src, dst, off, nv = Batch.concat(gs)
+    d_src, d_dst = torch.from_numpy(src).cuda(), torch.from_numpy(dst).cuda()
+    few_s, few_d = d_src.clone(), d_dst.clone()
+    a, z = int(off[1]), int(off[2])
+    few_s[a:z], few_d[a:z] = 1, 0
+    b = Batch(src=few_s, dst=few_d, offsets=off, num_vertices=nv, tile_cols=128)
+    assert b.count().tolist() == [want[0], 0]
+    tiles_few = b.info().bcsr.num_blocks
+    b.rebuild(src=d_src, dst=d_dst, offsets=off, num_vertices=nv, tile_cols=128, asynchronous=True)
+    out = torch.full((2,), 7, dtype=torch.int64, device="cuda")
+    b.count_async(out.data_ptr())
+    torch.cuda.synchronize()
+    assert out.cpu().tolist() == [0, 0]  # nothing built, nothing counted
+    with pytest.raises(BtcError) as e:
+        b.info()
+    assert e.value.status == _lib.BTC_E_CAPACITY
+    b.rebuild(src=d_src, dst=d_dst, offsets=off, num_vertices=nv, tile_cols=128)
+    assert b.count().tolist() == want
+    assert b.info().bcsr.num_blocks > tiles_few
+    b.free()
