@@ -721,9 +721,10 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
                             mma_b1(c1, a0, a1, b1);
                         }
                     } else {
-                        for (int k0 = 0; k0 < nm; k0 += 4) {
-                            const int k = k0 + tg;
-                            uint32_t a0 = 0, a1 = 0, b0 = 0, b1 = 0;
+                        // two packed groups' fragments are loaded before their four MMAs
+                        for (int k0 = 0; k0 < nm; k0 += 8) {
+                            const int k = k0 + tg, k2 = k0 + 4 + tg;
+                            uint32_t a0 = 0, a1 = 0, b0 = 0, b1 = 0, e0 = 0, e1 = 0, f0 = 0, f1 = 0;
                             if (k < nm) {
                                 const uint32_t* A = blocks + (size_t)s.mpa[k] * TW;
                                 const uint32_t* Bt = blocks + (size_t)s.mpb[k] * TW;
@@ -732,8 +733,20 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
                                 b0 = Bt[g];
                                 b1 = Bt[g + 8];
                             }
+                            if (k2 < nm) {
+                                const uint32_t* A = blocks + (size_t)s.mpa[k2] * TW;
+                                const uint32_t* Bt = blocks + (size_t)s.mpb[k2] * TW;
+                                e0 = A[g];
+                                e1 = A[g + 8];
+                                f0 = Bt[g];
+                                f1 = Bt[g + 8];
+                            }
                             mma_b1(c0, a0, a1, b0);
                             mma_b1(c1, a0, a1, b1);
+                            if (k0 + 4 < nm) {
+                                mma_b1(c0, e0, e1, f0);
+                                mma_b1(c1, e0, e1, f1);
+                            }
                         }
                     }
                     __syncwarp();
@@ -843,8 +856,10 @@ int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
     // rows at random, so what stays in L2 is what the warps in flight share; smaller
     // grabs keep those warps in fewer row blocks (measured on R-MAT scale 20 / 22 in
     // degree order, 16x128: 5.34 / 23.26 ms at 64 tiles, 2.80 / 21.91 ms at 16, 2.91 /
-    // 22.18 ms at 8).
-    const uint32_t chunk_rows = (uint32_t)(chunk_s < 16 ? chunk_s : 16);
+    // 22.18 ms at 8).  At least half an even share per warp, down to one tile: a graph
+    // of few, dense tiles (K_4096: 4224 tiles) keeps every warp busy.
+    uint64_t chunk_r = span / (warps * 2);
+    const uint32_t chunk_rows = (uint32_t)(chunk_r < 1 ? 1 : (chunk_r > 16 ? 16 : chunk_r));
     if (heavy && cellpp && row_off && row_ent && !tilewise)
         return launch_count_rows(tile_cols, indptr, indices, row_indices, blocks, num_tiles, tile_begin,
                                  tile_end, n_row_blocks, tau, chunk_rows, scr, graph_rows,

@@ -274,9 +274,12 @@ k_count_rows(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ i
                         mma_b1(c1, fa0, fa1, fb1);
                     }
                 } else {
-                    for (int k0 = 0; k0 < nm; k0 += 4) {
-                        const int k = k0 + tg;
-                        uint32_t fa0 = 0, fa1 = 0, fb0 = 0, fb1 = 0;
+                    // two packed groups' fragments are loaded before their four MMAs (for
+                    // 16x128 the same pairing measured slower: registers the sparse path
+                    // needs)
+                    for (int k0 = 0; k0 < nm; k0 += 8) {
+                        const int k = k0 + tg, k2 = k0 + 4 + tg;
+                        uint32_t fa0 = 0, fa1 = 0, fb0 = 0, fb1 = 0, ga0 = 0, ga1 = 0, gb0 = 0, gb1 = 0;
                         if (k < nm) {
                             const uint32_t* A = blocks + (size_t)s.mpa[k] * TW;
                             const uint32_t* Bt = blocks + (size_t)s.mpb[k] * TW;
@@ -285,8 +288,20 @@ k_count_rows(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ i
                             fb0 = Bt[fg];
                             fb1 = Bt[fg + 8];
                         }
+                        if (k2 < nm) {
+                            const uint32_t* A = blocks + (size_t)s.mpa[k2] * TW;
+                            const uint32_t* Bt = blocks + (size_t)s.mpb[k2] * TW;
+                            ga0 = A[fg];
+                            ga1 = A[fg + 8];
+                            gb0 = Bt[fg];
+                            gb1 = Bt[fg + 8];
+                        }
                         mma_b1(c0, fa0, fa1, fb0);
                         mma_b1(c1, fa0, fa1, fb1);
+                        if (k0 + 4 < nm) {
+                            mma_b1(c0, ga0, ga1, gb0);
+                            mma_b1(c1, ga0, ga1, gb1);
+                        }
                     }
                 }
                 __syncwarp();
