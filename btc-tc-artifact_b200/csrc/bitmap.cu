@@ -325,19 +325,33 @@ k_fill_bm(const int32_t* __restrict__ src, const int32_t* __restrict__ dst, int6
             word[k] = cp.x;
             pre[k] = cp.y;
         }
+        uint32_t tile[U];
 #pragma unroll
         for (int k = 0; k < U; ++k) {
-            if (!ok[k]) continue;
             const uint32_t below = (1u << ((c[k] >> LOG2C) & 31u)) - 1u;
-            const uint32_t t = pre[k] + __popc(word[k] & below);
-            const uint32_t cl = c[k] & (C - 1);
-            uint32_t* tw = &blocks[(size_t)t * TW + (r[k] & 15u) * WPR + (cl >> 5)];
-            if (rowmask) {
-                // the edge that finds its tile word empty marks the row: one mask atomic
-                // per non-empty word, none per edge of a busy row
-                if (atomicOr(tw, 1u << (cl & 31u)) == 0u) atomicOr(&rowmask[t], 1u << (r[k] & 15u));
-            } else {
-                atomicOr(tw, 1u << (cl & 31u));
+            tile[k] = pre[k] + __popc(word[k] & below);
+        }
+        if (rowmask) {
+            // the edge that finds its tile word empty marks the row: one mask atomic per
+            // non-empty word, none per edge of a busy row.  All U atomics are issued
+            // before the first old value is looked at.
+            uint32_t old[U];
+#pragma unroll
+            for (int k = 0; k < U; ++k) {
+                const uint32_t cl = c[k] & (C - 1);
+                old[k] = ok[k] ? atomicOr(&blocks[(size_t)tile[k] * TW + (r[k] & 15u) * WPR + (cl >> 5)],
+                                          1u << (cl & 31u))
+                               : 1u;
+            }
+#pragma unroll
+            for (int k = 0; k < U; ++k)
+                if (old[k] == 0u) atomicOr(&rowmask[tile[k]], 1u << (r[k] & 15u));
+        } else {
+#pragma unroll
+            for (int k = 0; k < U; ++k) {
+                if (!ok[k]) continue;
+                const uint32_t cl = c[k] & (C - 1);
+                atomicOr(&blocks[(size_t)tile[k] * TW + (r[k] & 15u) * WPR + (cl >> 5)], 1u << (cl & 31u));
             }
         }
     }

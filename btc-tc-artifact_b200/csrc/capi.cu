@@ -132,6 +132,15 @@ static bool row_index_possible(int64_t m, int32_t n_row_blocks)
     return n_row_blocks > 0 && m >= 8 * (int64_t)n_row_blocks && m < (int64_t)0xffffffffll;
 }
 
+static int reserve_row_index(btc_bitbsr* g, int64_t m, uint64_t R)
+{
+    BTC_TRY(g->row_off.reserve(sizeof(uint32_t) * (16 * R + 1)));
+    BTC_TRY(g->row_ent.reserve(sizeof(uint2) * (size_t)m));
+    BTC_TRY(g->row_tot.reserve(sizeof(uint32_t) * R));
+    return g->row_bsum.reserve(sizeof(unsigned long long) +
+                               sizeof(uint32_t) * ((size_t)ri_scan_blocks((uint32_t)R) + 1));
+}
+
 // The row index after the row masks (T = *d_tiles bounded by cap, or cap itself).
 static int enqueue_row_index(btc_bitbsr* g, const unsigned long long* d_tiles, uint32_t cap,
                              cudaStream_t s)
@@ -294,6 +303,11 @@ static int build_into(btc_bitbsr* g, const int32_t* src, const int32_t* dst, int
     BuildPlan P{};
     P.geom = make_geom(n, tile_cols);
     const BuildGeom& geom = P.geom;
+    // the previous build of this handle, when it had the same geometry, predicts whether
+    // the graph averages 8 or more tiles per row block (the row index's condition)
+    const bool prev_light = g->tile_cols == tile_cols && g->n_row_blocks == geom.n_row_blocks &&
+                            g->num_tiles > 0 &&
+                            (uint64_t)g->num_tiles < 8ull * (uint64_t)geom.n_row_blocks;
     g->tile_cols = tile_cols;
     g->n = n;
     g->n_row_blocks = geom.n_row_blocks;
@@ -345,16 +359,12 @@ static int build_into(btc_bitbsr* g, const int32_t* src, const int32_t* dst, int
         BTC_TRY(g->bitmap.reserve(sizeof(uint32_t) * (P.bm_words ? P.bm_words : 1)));
         BTC_TRY(g->prefix.reserve(sizeof(uint2) * (P.bm_words ? P.bm_words : 1)));
         // the row-wise count's row index: only a graph with at least 8 edges per row block
-        // can average 8 tiles per row block (every tile holds an edge)
-        P.row_index = row_index_possible(m, geom.n_row_blocks);
-        if (P.row_index) {
-            const uint64_t R = (uint64_t)geom.n_row_blocks;
-            BTC_TRY(g->row_off.reserve(sizeof(uint32_t) * (16 * R + 1)));
-            BTC_TRY(g->row_ent.reserve(sizeof(uint2) * (size_t)m));
-            BTC_TRY(g->row_tot.reserve(sizeof(uint32_t) * R));
-            BTC_TRY(g->row_bsum.reserve(sizeof(unsigned long long) +
-                                        sizeof(uint32_t) * ((size_t)ri_scan_blocks((uint32_t)R) + 1)));
-        }
+        // can average 8 tiles per row block (every tile holds an edge).  A rebuild whose
+        // previous graph of the same geometry averaged fewer skips it (a mesh would pay
+        // five launches that find nothing to do); should this graph average more after
+        // all, the count takes the tile-wise kernel, which needs no index.
+        P.row_index = row_index_possible(m, geom.n_row_blocks) && !prev_light;
+        if (P.row_index) BTC_TRY(reserve_row_index(g, m, (uint64_t)geom.n_row_blocks));
         g->row_index = P.row_index;
     }
     BTC_TRY(g->indptr.reserve(sizeof(uint32_t) * ((size_t)geom.n_row_blocks + 1)));
@@ -428,7 +438,15 @@ static int build_into(btc_bitbsr* g, const int32_t* src, const int32_t* dst, int
     BTC_TRY(launch_rowmask(tile_cols, g->blocks.as<uint32_t>(), g->num_tiles, nullptr,
                            g->indptr.as<uint32_t>(), g->n_row_blocks, g->rowmask.as<uint32_t>(),
                            meta + kMetaRowMax, s, !P.use_bitmap));
-    if (P.row_index) BTC_TRY(enqueue_row_index(g, nullptr, g->num_tiles, s));
+    // the tile count is known here: the index exactly when the graph averages 8 or more
+    // tiles per row block
+    P.row_index = P.use_bitmap && row_index_possible(m, geom.n_row_blocks) &&
+                  (uint64_t)g->num_tiles >= 8ull * (uint64_t)geom.n_row_blocks;
+    if (P.row_index) {
+        BTC_TRY(reserve_row_index(g, m, (uint64_t)geom.n_row_blocks));
+        BTC_TRY(enqueue_row_index(g, nullptr, g->num_tiles, s));
+    }
+    g->row_index = P.row_index;
     return BTC_OK;
 }
 
