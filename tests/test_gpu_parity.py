@@ -474,3 +474,33 @@ def test_compat_cli_reads_reference_bin_format(name, tmp_path):
         assert out.returncode == 0, out.stdout + out.stderr
         got = int(re.search(r"Triangles \(GPU\): (\d+)", out.stdout).group(1))
         assert got == fx["count"], (mode, out.stdout)
+
+
+def test_row_index_follows_the_graph_class():
+    """The row index (and with it the row-wise count) exists for graphs averaging 8 or more
+    tiles per row block.  An enqueued rebuild predicts that from the handle's previous
+    graph of the same geometry; alternating a mesh (a few tiles per row block) and a
+    random graph (dozens) on one handle, waiting and enqueued, must count exactly either
+    way -- a wrong prediction only changes which kernel counts."""
+    n = 4096
+    mesh = G.stencil27(16)                     # 16^3 = 4096 vertices, a few tiles per row block
+    rand = G.erdos_renyi(n, 32, seed=3)        # ~30 tiles per row block at 16x128
+    assert mesh[2] == n and rand[2] == n
+    want = {}
+    for key, (s, d, _) in (("mesh", mesh), ("rand", rand)):
+        rp, col, _ = O.lower_csr(s, d, n)
+        want[key] = O.tc_merge(rp, col)
+    g = BitBSR(_dev(mesh[0]), _dev(mesh[1]), n, 128)
+    assert g.count() == want["mesh"]
+    out = torch.zeros(1, dtype=torch.int64, device="cuda")
+    seq = ["rand", "rand", "mesh", "mesh", "rand", "mesh", "rand", "rand"]
+    for i, key in enumerate(seq):
+        s, d, _ = rand if key == "rand" else mesh
+        asynchronous = i % 3 != 2
+        g.rebuild(_dev(s), _dev(d), n, 128, asynchronous=asynchronous)
+        g.count_async(d_out=out.data_ptr())
+        assert int(out.item()) == want[key], (i, key, asynchronous)
+        assert g.count() == want[key], (i, key, asynchronous)
+        for tau in (0, _lib.BTC_TAU_ALL_SPARSE):
+            assert g.count(tau=tau) == want[key], (i, key, tau)
+    g.free()
