@@ -16,7 +16,9 @@ data-path collective).
   value      device-resident edge list in HBM, L2 flushed (512 MB write) before
              every timed step, CUDA events around each step, max over ranks
   e2e        the same through the public API with host buffers: H2D of the pinned
-             edge list, build, count, D2H of the count, every step
+             edge list, build, count, D2H of the count, every step; a stream of
+             steps on two handles and two streams, so one step's copy overlaps the
+             previous step's build and count (e2e.serial: one step at a time)
   roofline   the count kernel (dominant kernel of the step at this size) against
              the measured HBM copy bandwidth
   cpu_baseline   the reference's own cpu_tc_intersection_lower_triangular
@@ -863,6 +865,50 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_total = float(t.item())
 
+    # e2e over a stream of steps: consecutive steps alternate between two handles on two
+    # streams, so step i+1's copy from pinned host memory overlaps step i's build and
+    # count -- how a service counting a stream of graphs uses the API.  Every step still
+    # copies its whole edge list in and its count out; the inputs (537 MB a step) are
+    # larger than L2.  (Not with --shard, whose steps end in a collective.)
+    pipe = None
+    if not args.shard:
+        pipe_steps = max(2, e2e_steps - e2e_steps % 2)
+        s2 = torch.cuda.Stream()
+        g2 = BitBSR(np_src, np_dst, n, tile, orient_degree=odeg, stream=s2)
+        hs, sts = (g, g2), (stream, s2)
+        d_outs = torch.zeros(2, dtype=torch.int64, device="cuda")
+        h_outs = torch.zeros(pipe_steps, dtype=torch.int64).pin_memory()
+        for k in (0, 1):  # warm-up: both handles' enqueued rebuilds
+            hs[k].rebuild(np_src, np_dst, n, tile, orient_degree=odeg, stream=sts[k], asynchronous=True)
+            if hs[k].count(stream=sts[k]) != expected:
+                raise SystemExit("pipelined e2e warm-up count differs from the golden count")
+        torch.cuda.synchronize()
+        p0, p1, j2 = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+                      torch.cuda.Event())
+        p0.record(stream)
+        s2.wait_event(p0)
+        for i in range(pipe_steps):
+            k = i & 1
+            hs[k].rebuild(np_src, np_dst, n, tile, orient_degree=odeg, stream=sts[k], asynchronous=True)
+            hs[k].count_async(stream=sts[k], d_out=d_outs[k:k + 1].data_ptr())
+            with torch.cuda.stream(sts[k]):
+                h_outs[i:i + 1].copy_(d_outs[k:k + 1], non_blocking=True)
+        j2.record(s2)
+        stream.wait_event(j2)
+        p1.record(stream)
+        p1.synchronize()
+        bad = [int(x) for x in h_outs.tolist() if int(x) != expected]
+        if bad:
+            raise SystemExit(f"pipelined e2e counts {bad[:3]} != golden {expected}")
+        pipe_total = p0.elapsed_time(p1)
+        if dist:
+            t = torch.tensor([pipe_total], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            pipe_total = float(t.item())
+        pipe = (pipe_steps, pipe_total)
+        g2.free()
+        del d_outs
+
     # ---- roofline of the count kernel ----------------------------------------
     hbm, peak_src = peaks()
     bytes_count = 4 * (R + 1) + 8 * B + tw_bytes * B + 8
@@ -870,10 +916,10 @@ def main():
     achieved = bytes_count / tc / 1e9
     # DRAM bytes and warp instructions of one count launch on this workload, from the
     # committed ncu data (profiles/count_kernel.json; per launch, scaled from a smaller
-    # capture of the same graph family when the full size is too large to capture).  The
-    # kernel is issue-bound, so its warp-instruction rate against the SMs' (4 schedulers
-    # per SM, one warp instruction each per cycle, at the median SM clock sampled during
-    # the timed region) says how close it runs to its real limit.
+    # capture of the same graph family when the full size is too large to capture).  Its
+    # warp-instruction rate against the SMs' (4 schedulers per SM, one warp instruction
+    # each per cycle, at the median SM clock sampled during the timed region) is the
+    # issue side of the bound; dependent-load latency is the other.
     prof = count_profile(args.workload, tile)
     traffic = int(prof["dram_bytes_per_launch"]) if prof else None
     warp_inst = float(prof["warp_instructions_per_launch"]) if prof else None
@@ -909,8 +955,17 @@ def main():
                    "parallelism": (f"tile-sharded x{world}, int64 all-reduce" if args.shard
                                    else f"replica x{world}" if world > 1 else "single GPU"),
                    "l2": "flushed before every timed step (512 MB write)"},
-        "e2e": {"value": jobs * m_lower * e2e_steps / (e2e_total / 1e3), "unit": UNIT,
-                "h2d_bytes_per_step": 8 * m_in, "d2h_bytes_per_step": 8 + 24},
+        "e2e": ({"value": jobs * m_lower * pipe[0] / (pipe[1] / 1e3), "unit": UNIT,
+                 "h2d_bytes_per_step": 8 * m_in, "d2h_bytes_per_step": 8 + 24, "steps": pipe[0],
+                 "ms_per_step": pipe[1] / pipe[0],
+                 "how": "stream of steps on two handles and two streams (step i+1's H2D "
+                        "overlaps step i's build and count)",
+                 "serial": {"value": jobs * m_lower * e2e_steps / (e2e_total / 1e3),
+                            "ms_per_step": e2e_total / e2e_steps,
+                            "how": "one step at a time: H2D, build, count, count back"}}
+                if pipe else
+                {"value": jobs * m_lower * e2e_steps / (e2e_total / 1e3), "unit": UNIT,
+                 "h2d_bytes_per_step": 8 * m_in, "d2h_bytes_per_step": 8 + 24}),
         "gpu_launches": launches_per_step(n, tile, odeg, m_in) * args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": traffic,

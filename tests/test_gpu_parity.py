@@ -490,10 +490,11 @@ def test_row_index_follows_the_graph_class():
     for key, (s, d, _) in (("mesh", mesh), ("rand", rand)):
         rp, col, _ = O.lower_csr(s, d, n)
         want[key] = O.tc_merge(rp, col)
-    g = BitBSR(_dev(mesh[0]), _dev(mesh[1]), n, 128)
-    assert g.count() == want["mesh"]
+    # the random graph first: its tile arrays have room for every later enqueued rebuild
+    g = BitBSR(_dev(rand[0]), _dev(rand[1]), n, 128)
+    assert g.count() == want["rand"]
     out = torch.zeros(1, dtype=torch.int64, device="cuda")
-    seq = ["rand", "rand", "mesh", "mesh", "rand", "mesh", "rand", "rand"]
+    seq = ["mesh", "mesh", "rand", "rand", "mesh", "rand", "mesh", "rand", "rand"]
     for i, key in enumerate(seq):
         s, d, _ = rand if key == "rand" else mesh
         asynchronous = i % 3 != 2
