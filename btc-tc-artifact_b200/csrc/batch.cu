@@ -507,6 +507,22 @@ size_t batch_device_bytes(const btc_batch* b)
 }
 }  // namespace btc200
 
+namespace btc200 {
+// An empty batch whose allocations are all stream-ordered on `s` from `pool` (see
+// bitbsr_new_pooled); its first (re)build sizes it.
+btc_batch* batch_new_pooled(cudaMemPool_t pool, cudaStream_t s)
+{
+    btc_batch* b = new (std::nothrow) btc_batch();
+    if (!b) return nullptr;
+    b->g.set_pool(pool, s);
+    for (DevBuf* d : {&b->segs, &b->e_off, &b->bm_off, &b->row_off, &b->counts}) {
+        d->pool = pool;
+        d->stream = s;
+    }
+    return b;
+}
+}  // namespace btc200
+
 extern "C" {
 
 int btc_batch_build(const int32_t* src, const int32_t* dst, const int64_t* edge_offsets,

@@ -78,11 +78,11 @@ int ensure_count_scratch(btc_bitbsr* g)
     if (g->partials.bytes < need) BTC_TRY(g->partials.reserve(need));
     if (!g->done.ptr) {
         BTC_TRY(g->done.reserve(kCountCtlBytes));
-        BTC_CUDA_TRY(cudaMemset(g->done.ptr, 0, kCountCtlBytes));
+        BTC_CUDA_TRY(g->done.zero(kCountCtlBytes));
     }
     if (!g->result.ptr) {
         BTC_TRY(g->result.reserve(sizeof(unsigned long long)));
-        BTC_CUDA_TRY(cudaMemset(g->result.ptr, 0, sizeof(unsigned long long)));
+        BTC_CUDA_TRY(g->result.zero(sizeof(unsigned long long)));
     }
     return BTC_OK;
 }
@@ -503,6 +503,17 @@ int resolve_build(btc_bitbsr* g)
 // ===========================================================================
 // C ABI
 // ===========================================================================
+namespace btc200 {
+// An empty handle whose allocations are all stream-ordered on `s` from `pool`, for an
+// owner that uses it on `s` only (a server slot); its first (re)build sizes it.
+btc_bitbsr* bitbsr_new_pooled(cudaMemPool_t pool, cudaStream_t s)
+{
+    btc_bitbsr* g = new (std::nothrow) btc_bitbsr();
+    if (g) g->set_pool(pool, s);
+    return g;
+}
+}  // namespace btc200
+
 extern "C" {
 
 int btc_abi_version(void) { return (1 << 16) | 0; }

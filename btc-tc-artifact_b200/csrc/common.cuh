@@ -63,19 +63,22 @@ __host__ __device__ __forceinline__ int log2_exact(int x)
 struct DevBuf {
     void* ptr = nullptr;
     size_t bytes = 0;
+    // Stream-ordered allocation, for an owner that uses the buffer on one stream only:
+    // with `pool` and `stream` set, a growth frees and allocates in that stream's order
+    // (cudaFreeAsync / cudaMallocFromPoolAsync) instead of cudaFree's wait for the whole
+    // device.  `pooled` records how the current allocation was made.
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t stream = nullptr;
+    bool pooled = false;
     int reserve(size_t need)
     {
         if (need <= bytes && ptr) return BTC_OK;
-        if (ptr) cudaFree(ptr);
-        ptr = nullptr;
-        bytes = 0;
+        release();
         if (need == 0) return BTC_OK;
         size_t want = need + need / 8;  // headroom for slowly growing rebuilds
-        cudaError_t e = cudaMalloc(&ptr, want);
-        if (e != cudaSuccess) {
+        if (allocate(want) != cudaSuccess) {
             cudaGetLastError();
-            e = cudaMalloc(&ptr, need);
-            if (e != cudaSuccess) {
+            if (allocate(need) != cudaSuccess) {
                 cudaGetLastError();
                 ptr = nullptr;
                 return BTC_E_NOMEM;
@@ -85,11 +88,24 @@ struct DevBuf {
         bytes = want;
         return BTC_OK;
     }
+    cudaError_t allocate(size_t b)
+    {
+        pooled = pool != nullptr && stream != nullptr;
+        return pooled ? cudaMallocFromPoolAsync(&ptr, b, pool, stream) : cudaMalloc(&ptr, b);
+    }
     void release()
     {
-        if (ptr) cudaFree(ptr);
+        if (ptr) {
+            if (pooled) cudaFreeAsync(ptr, stream);
+            else cudaFree(ptr);
+        }
         ptr = nullptr;
         bytes = 0;
+    }
+    // zeroes the first n bytes, ordered with the buffer's stream when it has one
+    cudaError_t zero(size_t n) const
+    {
+        return pooled ? cudaMemsetAsync(ptr, 0, n, stream) : cudaMemset(ptr, 0, n);
     }
     template <class T>
     T* as() const { return static_cast<T*>(ptr); }

@@ -49,23 +49,33 @@ struct btc_bitbsr {
     BuildGraphKey last_key{};
     cudaStream_t capture_stream = nullptr;
 
+    template <class F>
+    void for_each_buf(F f)
+    {
+        btc200::DevBuf* all[] = {&indptr, &indices, &row_indices, &blocks, &result, &in_src, &in_dst,
+                                 &keys0, &keys1, &sort_scratch, &tile_base, &meta, &deg, &rank,
+                                 &bitmap, &prefix, &partials, &done, &rowmask, &row_off, &row_ent,
+                                 &row_tot, &row_bsum};
+        for (btc200::DevBuf* b : all) f(*b);
+    }
     size_t device_bytes() const
     {
-        const btc200::DevBuf* all[] = {&indptr, &indices, &row_indices, &blocks, &result, &in_src, &in_dst,
-                               &keys0, &keys1, &sort_scratch, &tile_base, &meta, &deg, &rank,
-                               &bitmap, &prefix, &partials, &done, &rowmask, &row_off, &row_ent,
-                               &row_tot, &row_bsum};
         size_t s = 0;
-        for (const btc200::DevBuf* b : all) s += b->bytes;
+        const_cast<btc_bitbsr*>(this)->for_each_buf([&](btc200::DevBuf& b) { s += b.bytes; });
         return s;
+    }
+    // every later allocation of this handle is stream-ordered on `s` from `pool` (the
+    // handle is then used on `s` only)
+    void set_pool(cudaMemPool_t pool, cudaStream_t s)
+    {
+        for_each_buf([&](btc200::DevBuf& b) {
+            b.pool = pool;
+            b.stream = s;
+        });
     }
     void release_all()
     {
-        btc200::DevBuf* all[] = {&indptr, &indices, &row_indices, &blocks, &result, &in_src, &in_dst,
-                         &keys0, &keys1, &sort_scratch, &tile_base, &meta, &deg, &rank,
-                         &bitmap, &prefix, &partials, &done, &rowmask, &row_off, &row_ent,
-                         &row_tot, &row_bsum};
-        for (btc200::DevBuf* b : all) b->release();
+        for_each_buf([](btc200::DevBuf& b) { b.release(); });
         if (h_meta) cudaFreeHost(h_meta);
         h_meta = nullptr;
         d_hmeta = nullptr;

@@ -15,11 +15,15 @@
 // nothing for it, and degree order keeps its hub rows short) once it reaches the front
 // of the queue; a batch being formed passes over such requests and takes the small ones
 // behind them.  Solo rebuilds are enqueued without a host wait, so the engine thread
-// keeps filling the other slots meanwhile.  All slots share one solo handle, one solo
-// launch at a time: the handle's buffers grow to the largest request once, instead of
-// once per slot (a growth frees and allocates device memory, which waits for every
-// stream, the other slots' batches included).  With slots = 1 and max_batch_graphs = 1
-// the same server is the plain one-request-at-a-time path.
+// keeps filling the other slots meanwhile.  One solo launch runs at a time, on whichever
+// slot takes it, through one solo handle: a large graph occupies the whole GPU, so two
+// at once would gain nothing and would hold both slots while small requests wait.  Every
+// device allocation (batch and solo handles, edge copies) is stream-ordered on the
+// stream of the slot using it, from a pool the server owns: a handle that grows for a
+// larger request frees and allocates without cudaFree's wait for the whole device, so
+// one slot's growth never stalls the engine behind another slot's long batch.  With
+// slots = 1 and max_batch_graphs = 1 the same server is the plain one-request-at-a-time
+// path.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -36,6 +40,8 @@
 
 namespace btc200 {
 size_t batch_device_bytes(const btc_batch* b);
+btc_bitbsr* bitbsr_new_pooled(cudaMemPool_t pool, cudaStream_t s);
+btc_batch* batch_new_pooled(cudaMemPool_t pool, cudaStream_t s);
 }
 
 namespace {
@@ -104,6 +110,7 @@ struct btc_server {
     std::deque<Request> pending;
     std::vector<btc_server_result> done;
     std::vector<Slot> slots;
+    cudaMemPool_t pool = nullptr;  // the slots' device memory (stream-ordered)
     // large requests: one graph, descending-degree order, on whichever slot runs it
     btc_bitbsr* solo = nullptr;
     int solo_slot = -1;        // the slot whose launch holds the solo handle, or -1
@@ -240,25 +247,21 @@ int launch_slot(btc_server* s, Slot& sl)
         // Rebuilds are enqueued without a host wait (BTC_BUILD_ASYNC), so the engine
         // thread goes on filling the other slots; finish_solo checks the build's status.
         // The admission loop handed this slot the solo handle (s->solo_slot); the slot
-        // that used it before has been published, so its stream is done with it.
-        if (!s->solo) {
-            st = btc_build_bitbsr(ds, dd, m, sl.reqs[0].n, 0, BTC_ORIENT_DEGREE, sl.stream,
-                                  &s->solo);
-        } else {
-            st = btc_rebuild_bitbsr(s->solo, ds, dd, m, sl.reqs[0].n, 0,
-                                    BTC_ORIENT_DEGREE | BTC_BUILD_ASYNC, sl.stream);
-            s->solo_async = st == BTC_OK;
-        }
+        // that ran it before has been published, so no stream still uses its buffers, and
+        // its allocations now follow this slot's stream.  (The first build into the empty
+        // handle waits: there are no arrays to enqueue against yet.)
+        if (!s->solo && !(s->solo = btc200::bitbsr_new_pooled(s->pool, sl.stream))) return BTC_E_NOMEM;
+        s->solo->set_pool(s->pool, sl.stream);
+        st = btc_rebuild_bitbsr(s->solo, ds, dd, m, sl.reqs[0].n, 0,
+                                BTC_ORIENT_DEGREE | BTC_BUILD_ASYNC, sl.stream);
+        s->solo_async = st == BTC_OK;
         if (st != BTC_OK) return st;
         st = btc_count_async(s->solo, s->cfg.tau, sl.stream, sl.d_counts.as<unsigned long long>());
         if (st != BTC_OK) return st;
     } else {
-        if (!sl.batch)
-            st = btc_batch_build(ds, dd, sl.offsets.data(), sl.nv.data(), G, s->cfg.tile_cols, 0,
-                                 sl.stream, &sl.batch);
-        else
-            st = btc_batch_rebuild(sl.batch, ds, dd, sl.offsets.data(), sl.nv.data(), G,
-                                   s->cfg.tile_cols, 0, sl.stream);
+        if (!sl.batch && !(sl.batch = btc200::batch_new_pooled(s->pool, sl.stream))) return BTC_E_NOMEM;
+        st = btc_batch_rebuild(sl.batch, ds, dd, sl.offsets.data(), sl.nv.data(), G,
+                               s->cfg.tile_cols, 0, sl.stream);
         if (st != BTC_OK) return st;
         st = btc_batch_count(sl.batch, s->cfg.tau, sl.stream,
                              sl.d_counts.as<unsigned long long>(), nullptr);
@@ -461,6 +464,20 @@ int btc_server_create(const btc_server_config* cfg, btc_server** out)
         delete s;
         return BTC_E_CUDA;
     }
+    // the slots' device memory: a pool that keeps what is freed for the next request
+    // (the HBM budget bounds what the slots hold)
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = s->device;
+    uint64_t keep = ~0ull;
+    if (cudaMemPoolCreate(&s->pool, &props) != cudaSuccess ||
+        cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) {
+        cudaGetLastError();
+        if (s->pool) cudaMemPoolDestroy(s->pool);
+        delete s;
+        return BTC_E_CUDA;
+    }
     s->slots.resize((size_t)cfg->slots);
     for (Slot& sl : s->slots) {
         if (cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) != cudaSuccess ||
@@ -471,8 +488,13 @@ int btc_server_create(const btc_server_config* cfg, btc_server** out)
                 if (o.start) cudaEventDestroy(o.start);
                 if (o.done) cudaEventDestroy(o.done);
             }
+            cudaMemPoolDestroy(s->pool);
             delete s;
             return BTC_E_CUDA;
+        }
+        for (btc200::DevBuf* d : {&sl.d_counts, &sl.d_src, &sl.d_dst}) {
+            d->pool = s->pool;
+            d->stream = sl.stream;
         }
     }
     s->engine = std::thread(engine_loop, s);
@@ -539,6 +561,8 @@ void btc_server_destroy(btc_server* s)
         s->cv.notify_all();
     }
     if (s->engine.joinable()) s->engine.join();
+    // the handles' and buffers' frees are ordered on the slot streams: free, then let the
+    // streams drain, then drop the streams and the pool
     if (s->solo) btc_free(s->solo);
     for (Slot& sl : s->slots) {
         if (sl.batch) btc_batch_free(sl.batch);
@@ -548,10 +572,14 @@ void btc_server_destroy(btc_server* s)
         sl.h_src.release();
         sl.h_dst.release();
         sl.h_counts.release();
+        if (sl.stream) cudaStreamSynchronize(sl.stream);
+    }
+    for (Slot& sl : s->slots) {
         if (sl.stream) cudaStreamDestroy(sl.stream);
         if (sl.start) cudaEventDestroy(sl.start);
         if (sl.done) cudaEventDestroy(sl.done);
     }
+    if (s->pool) cudaMemPoolDestroy(s->pool);
     delete s;
 }
 

@@ -384,7 +384,9 @@ BTC_API void btc_server_default_config(btc_server_config* cfg);
 
 /* Starts a server on the current device.  A batch slot admits queued requests in
  * arrival order while the batch stays within the caps and all slots stay within the
- * budget; requests that arrive while batches are on the GPU join the next batch. */
+ * budget; requests that arrive while batches are on the GPU join the next batch.  The
+ * slots' device memory comes from a stream-ordered pool the server owns (freed memory
+ * stays in the pool for later requests until btc_server_destroy). */
 BTC_API int btc_server_create(const btc_server_config* cfg, btc_server** out);
 
 /* Host-side allocation-failure injection, for tests of the server's recovery: when the
