@@ -477,7 +477,10 @@ int count_handle(btc_bitbsr* g, int tau, cudaStream_t s, unsigned long long* d_o
                         g->meta.as<unsigned long long>() + kMetaRowMax, tile_begin, tile_end,
                         build_meta, g->num_tiles,
                         g->used_bitmap && g->row_index ? g->row_off.as<uint32_t>() : nullptr,
-                        g->used_bitmap && g->row_index ? g->row_ent.as<uint2>() : nullptr);
+                        g->used_bitmap && g->row_index ? g->row_ent.as<uint2>() : nullptr,
+                        // tiles averaging more than half of tau's bits: the kernel variant
+                        // that keeps the tensor-core path's registers
+                        (uint64_t)g->input_edges * 2 > (uint64_t)tau * (uint64_t)g->num_tiles);
 }
 
 int resolve_build(btc_bitbsr* g)

@@ -174,7 +174,8 @@ int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
                  uint64_t cell_wpr = 0, const unsigned long long* row_max = nullptr,
                  uint32_t tile_begin = 0, uint32_t tile_end = 0xffffffffu,
                  const unsigned long long* build_meta = nullptr, uint32_t tiles_hint = 0,
-                 const uint32_t* row_off = nullptr, const uint2* row_ent = nullptr);
+                 const uint32_t* row_off = nullptr, const uint2* row_ent = nullptr,
+                 bool dense_tiles = false);
 
 // rowmask[t] bit r = tile t's row r has a bit, for t < T = *d_tiles (T = cap when d_tiles
 // is null) when T >= 8 * n_row_blocks (the heavy count variant's condition), and

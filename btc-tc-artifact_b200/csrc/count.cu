@@ -787,10 +787,9 @@ k_count(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indice
 
 }  // namespace
 
-// Persistent grid of the count kernel: resident CTAs per SM (the same for every variant:
-// 256 threads at 64 registers and the same shared memory) times the SMs; cached per
-// device and tile width.
-int count_grid_size(int tile_cols)
+// Resident CTAs per SM of the tile-wise kernel (the same for both variants: 256 threads
+// at 64 registers and the same shared memory), cached per device and tile width.
+static int tile_blocks_per_sm(int tile_cols)
 {
     static std::atomic<int> cache[64][2];
     int dev = 0;
@@ -807,9 +806,18 @@ int count_grid_size(int tile_cols)
     else
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_count<32, false>, kThreads, 0);
     if (e != cudaSuccess || per_sm < 1) per_sm = 1;
-    const int grid = per_sm * device_sm_count();
-    if (dev >= 0 && dev < 64) cache[dev][w].store(grid, std::memory_order_relaxed);
-    return grid;
+    if (dev >= 0 && dev < 64) cache[dev][w].store(per_sm, std::memory_order_relaxed);
+    return per_sm;
+}
+
+// Persistent grid of the count kernels: the larger of the two kernels' resident CTAs
+// per SM, times the SMs (the CTAs a count's scratch holds a partial sum for; each
+// launch runs at most its own kernel's resident CTAs).
+int count_grid_size(int tile_cols)
+{
+    const int rows = rows_blocks_per_sm(tile_cols);
+    const int tile = tile_blocks_per_sm(tile_cols);
+    return (rows > tile ? rows : tile) * device_sm_count();
 }
 
 int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
@@ -819,14 +827,16 @@ int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
                  const uint32_t* rowmask, const uint2* cellpp,
                  uint64_t cell_wpr, const unsigned long long* row_max, uint32_t tile_begin,
                  uint32_t tile_end, const unsigned long long* build_meta, uint32_t tiles_hint,
-                 const uint32_t* row_off, const uint2* row_ent)
+                 const uint32_t* row_off, const uint2* row_ent, bool dense_tiles)
 {
     // build_meta: num_tiles is a capacity bound and the kernel reads the device tile
     // count; the schedule and the variant follow tiles_hint (the previous build's count)
     if (tile_end > num_tiles) tile_end = num_tiles;
     if (tile_begin > tile_end) tile_begin = tile_end;
     const uint32_t span = build_meta ? min(tiles_hint, tile_end - tile_begin) : tile_end - tile_begin;
-    const int grid = count_grid_size(tile_cols);
+    const int grid_all = count_grid_size(tile_cols);
+    const int grid_tile = tile_blocks_per_sm(tile_cols) * device_sm_count();
+    const int grid = grid_tile < grid_all ? grid_tile : grid_all;
     // Guided schedule: the first round of grabs is about half of an even share per warp
     // (2 to 64 tiles; later rounds halve it down to 2: a one-tile grab costs a contended
     // queue atomic per tile).  Fixed schedule: about an eighth of an even share (8 to 64 tiles);
@@ -864,7 +874,7 @@ int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
         return launch_count_rows(tile_cols, indptr, indices, row_indices, blocks, num_tiles, tile_begin,
                                  tile_end, n_row_blocks, tau, chunk_rows, scr, graph_rows,
                                  num_graphs, graph_counts, rowmask, cellpp, cell_wpr, row_off, row_ent,
-                                 build_meta, grid, s);
+                                 build_meta, dense_tiles, grid_all, s);
 #define BTC_LAUNCH_COUNT(CC, HH)                                                              \
     k_count<CC, HH><<<grid, kThreads, 0, s>>>(indptr, indices, row_indices, blocks, num_tiles, \
                                               tile_begin, tile_end, n_row_blocks, tau,         \

@@ -136,6 +136,9 @@ __device__ __forceinline__ void finish_count(unsigned long long acc, CountScratc
     }
 }
 
+// Resident CTAs per SM of the row-wise kernel (count_rows.cu); 0 on error.
+int rows_blocks_per_sm(int tile_cols);
+
 // The row-wise count kernel (count_rows.cu), launched by launch_count for heavy graphs.
 int launch_count_rows(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
                       const uint32_t* row_indices, const uint32_t* blocks, uint32_t num_tiles,
@@ -144,6 +147,6 @@ int launch_count_rows(int tile_cols, const uint32_t* indptr, const uint32_t* ind
                       uint32_t num_graphs, unsigned long long* graph_counts,
                       const uint32_t* rowmask, const uint2* cellpp, uint64_t cell_wpr,
                       const uint32_t* row_off, const uint2* row_ent,
-                      const unsigned long long* build_meta, int grid, cudaStream_t s);
+                      const unsigned long long* build_meta, bool dense, int grid, cudaStream_t s);
 
 }  // namespace btc200

@@ -66,8 +66,12 @@ static_assert(kGCap == 64, "the group search below takes six steps");
 template <int C>
 constexpr size_t rows_smem_bytes() { return sizeof(RowSmem<C>) * kRWarps; }
 
-template <int C>
-__global__ void __launch_bounds__(kRThreads, 4)
+// kMinBlocks: resident CTAs per SM the registers are capped for.  Sparse 16x128 graphs
+// take five (48 registers; R-MAT s22 20.85 ms against 21.89 at four: the dependent-load
+// chains want every warp they can get), graphs of dense 16x128 tiles four (64 registers:
+// K_4096 on the tensor-core path 0.19 ms against 0.23 at five), 16x32 four.
+template <int C, int kMinBlocks>
+__global__ void __launch_bounds__(kRThreads, kMinBlocks)
 k_count_rows(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
              const uint32_t* __restrict__ row_indices, const uint32_t* __restrict__ blocks,
              uint32_t num_tiles, uint32_t tile_begin, uint32_t tile_end, int32_t R, int tau,
@@ -440,7 +444,48 @@ k_count_rows(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ i
     finish_count<kRThreads>(acc, scr, build_failed, s_red, &s_last);
 }
 
+
+using RowsKernel = decltype(&k_count_rows<128, 5>);
+
+// variant 0: 16x128 sparse, 1: 16x128 dense, 2: 16x32
+RowsKernel rows_kernel(int v)
+{
+    return v == 0 ? k_count_rows<128, 5> : v == 1 ? k_count_rows<128, 4> : k_count_rows<32, 4>;
+}
+
+int rows_variant(int tile_cols, bool dense) { return tile_cols == 128 ? (dense ? 1 : 0) : 2; }
+
+// Resident CTAs per SM of a row-wise kernel variant (dynamic shared memory above 48 KB is
+// an opt-in per function, set here once per device); 0 on error.
+int rows_variant_blocks_per_sm(int v)
+{
+    static std::atomic<int> resident[64][3];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+    int per_sm = resident[dev][v].load(std::memory_order_acquire);
+    if (per_sm > 0) return per_sm;
+    const size_t smem = v == 2 ? rows_smem_bytes<32>() : rows_smem_bytes<128>();
+    const RowsKernel k = rows_kernel(v);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kRThreads, smem);
+    if (e != cudaSuccess || per_sm < 1) {
+        note_cuda_error(e, "k_count_rows launch set-up", __FILE__, __LINE__);
+        return 0;
+    }
+    resident[dev][v].store(per_sm, std::memory_order_release);
+    return per_sm;
+}
+
 }  // namespace
+
+// Resident CTAs per SM of the row-wise kernel: the most any of its variants for this tile
+// width runs (what a count's scratch must hold partial sums for); 0 on error.
+int rows_blocks_per_sm(int tile_cols)
+{
+    const int a = rows_variant_blocks_per_sm(rows_variant(tile_cols, false));
+    const int b = rows_variant_blocks_per_sm(rows_variant(tile_cols, true));
+    return a > b ? a : b;
+}
 
 int launch_count_rows(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
                       const uint32_t* row_indices, const uint32_t* blocks, uint32_t num_tiles,
@@ -449,45 +494,19 @@ int launch_count_rows(int tile_cols, const uint32_t* indptr, const uint32_t* ind
                       uint32_t num_graphs, unsigned long long* graph_counts,
                       const uint32_t* rowmask, const uint2* cellpp, uint64_t cell_wpr,
                       const uint32_t* row_off, const uint2* row_ent,
-                      const unsigned long long* build_meta, int grid, cudaStream_t s)
+                      const unsigned long long* build_meta, bool dense, int grid, cudaStream_t s)
 {
-    // Dynamic shared memory above 48 KB is an opt-in per function, set once per device,
-    // and the persistent grid is this kernel's resident CTAs, at most `grid` (the CTAs
-    // the caller's scratch holds a partial sum for).
-    static std::atomic<int> resident[64][2];
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return BTC_E_CUDA;
-    const int w = tile_cols == 128 ? 0 : 1;
-    const size_t smem = tile_cols == 128 ? rows_smem_bytes<128>() : rows_smem_bytes<32>();
-    int per_sm = resident[dev][w].load(std::memory_order_acquire);
-    if (per_sm == 0) {
-        cudaError_t e;
-        if (tile_cols == 128) {
-            e = cudaFuncSetAttribute(k_count_rows<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e == cudaSuccess)
-                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_count_rows<128>, kRThreads, smem);
-        } else {
-            e = cudaFuncSetAttribute(k_count_rows<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e == cudaSuccess)
-                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_count_rows<32>, kRThreads, smem);
-        }
-        if (e != cudaSuccess || per_sm < 1) {
-            note_cuda_error(e, "k_count_rows launch set-up", __FILE__, __LINE__);
-            return BTC_E_CUDA;
-        }
-        resident[dev][w].store(per_sm, std::memory_order_release);
-    }
+    // the persistent grid is this kernel's resident CTAs, at most `grid` (the CTAs the
+    // caller's scratch holds a partial sum for)
+    const int v = rows_variant(tile_cols, dense);
+    const size_t smem = v == 2 ? rows_smem_bytes<32>() : rows_smem_bytes<128>();
+    const int per_sm = rows_variant_blocks_per_sm(v);
+    if (per_sm < 1) return BTC_E_CUDA;
     if (per_sm * device_sm_count() < grid) grid = per_sm * device_sm_count();
-    if (tile_cols == 128)
-        k_count_rows<128><<<grid, kRThreads, smem, s>>>(indptr, indices, row_indices, blocks, num_tiles,
-                                                        tile_begin, tile_end, n_row_blocks, tau, chunk, scr,
-                                                        graph_rows, num_graphs, graph_counts, rowmask,
-                                                        cellpp, cell_wpr, row_off, row_ent, build_meta);
-    else
-        k_count_rows<32><<<grid, kRThreads, smem, s>>>(indptr, indices, row_indices, blocks, num_tiles,
-                                                       tile_begin, tile_end, n_row_blocks, tau, chunk, scr,
-                                                       graph_rows, num_graphs, graph_counts, rowmask,
-                                                       cellpp, cell_wpr, row_off, row_ent, build_meta);
+    rows_kernel(v)<<<grid, kRThreads, smem, s>>>(indptr, indices, row_indices, blocks, num_tiles,
+                                                 tile_begin, tile_end, n_row_blocks, tau, chunk, scr,
+                                                 graph_rows, num_graphs, graph_counts, rowmask,
+                                                 cellpp, cell_wpr, row_off, row_ent, build_meta);
     return cudaGetLastError() == cudaSuccess ? BTC_OK : BTC_E_CUDA;
 }
 
