@@ -283,8 +283,9 @@ k_bm_emit(const uint32_t* __restrict__ bitmap, uint64_t W, uint64_t wpr,
     }
 }
 
+// six CTAs per SM (40 registers): R-MAT s22 build 9.38 ms against 9.51 at the default five
 template <int LOG2C>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 6)
 k_fill_bm(const int32_t* __restrict__ src, const int32_t* __restrict__ dst, int64_t m, int32_t n,
           const int32_t* __restrict__ rank, uint64_t wpr, const uint32_t* __restrict__ bitmap,
           const uint2* __restrict__ cellpp, uint32_t* __restrict__ blocks,
