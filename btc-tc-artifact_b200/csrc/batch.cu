@@ -22,16 +22,6 @@
 
 namespace btc200 {
 
-struct GraphSeg {
-    uint32_t row_off;  // first global row block
-    int32_t n;         // vertices (local ids are in [0, n))
-    uint32_t vbase;    // first global vertex id (16 * row_off)
-    uint32_t cb_lo;    // first global column block of the graph's vertex range
-    uint32_t wpr;      // bitmap words per row block
-    uint32_t pad;
-    uint64_t bm_off;   // first bitmap word of the graph
-};
-
 namespace bt {
 
 constexpr int kThreads = 256;
@@ -98,7 +88,7 @@ k_mark_b(const int32_t* __restrict__ src, const int32_t* __restrict__ dst, int64
 __global__ void __launch_bounds__(kThreads)
 k_emit_b(const uint32_t* __restrict__ bitmap, uint64_t W, const GraphSeg* __restrict__ segs,
          const uint64_t* __restrict__ bm_off, uint32_t G, const uint32_t* __restrict__ chunk_base,
-         uint32_t* __restrict__ prefix, uint32_t* __restrict__ indices,
+         uint2* __restrict__ cellpp, uint32_t* __restrict__ indices,
          uint32_t* __restrict__ row_indices, uint32_t* __restrict__ indptr,
          const unsigned long long* __restrict__ tiles, uint32_t cap, uint4* __restrict__ blocks,
          uint32_t tile_vec4)
@@ -148,7 +138,7 @@ k_emit_b(const uint32_t* __restrict__ bitmap, uint64_t W, const GraphSeg* __rest
             rb = 0;
             cw = 0;
         }
-        prefix[w] = base;
+        cellpp[w] = make_uint2(x[k], base);
         if (cw == 0) indptr[s.row_off + rb] = base;
         uint32_t bits = x[k];
         while (bits) {
@@ -169,8 +159,8 @@ template <int LOG2C>
 __global__ void __launch_bounds__(kThreads)
 k_fill_b(const int32_t* __restrict__ src, const int32_t* __restrict__ dst, int64_t m,
          const GraphSeg* __restrict__ segs, const int64_t* __restrict__ e_off, uint32_t G,
-         const uint32_t* __restrict__ bitmap, const uint32_t* __restrict__ prefix,
-         uint32_t* __restrict__ blocks, const unsigned long long* __restrict__ tiles, uint32_t cap)
+         const uint2* __restrict__ cellpp, uint32_t* __restrict__ blocks,
+         const unsigned long long* __restrict__ tiles, uint32_t cap)
 {
     if (*tiles > cap) return;  // nothing was emitted
     constexpr int C = 1 << LOG2C;
@@ -183,7 +173,8 @@ k_fill_b(const int32_t* __restrict__ src, const int32_t* __restrict__ dst, int64
         bool bad;
         if (!local_edge(src, dst, i, s, r, c, bad)) continue;
         const uint64_t w = cell_word<LOG2C>(s, r, c, bit);
-        const uint32_t t = prefix[w] + __popc(bitmap[w] & (bit - 1u));
+        const uint2 cp = cellpp[w];
+        const uint32_t t = cp.y + __popc(cp.x & (bit - 1u));
         const uint32_t cl = (s.vbase + c) & (C - 1);
         atomicOr(&blocks[(size_t)t * TW + (r & 15u) * WPR + (cl >> 5)], 1u << (cl & 31u));
     }
@@ -217,6 +208,7 @@ struct btc_batch {
     std::vector<uint32_t> h_rowoff;
     std::vector<int32_t> h_nv;
     bool built = false;        // the geometry above belongs to a build that succeeded
+    bool row_index = false;    // the builds enqueue the row index (row-wise count)
     bool pending = false;      // an enqueued rebuild's status is not known yet
     uint32_t pending_cap = 0;  // the tile capacity that rebuild ran against
     cudaStream_t pending_stream = nullptr;
@@ -268,9 +260,11 @@ static uint32_t batch_capacity(const btc_batch* b)
     return (uint32_t)std::min<uint64_t>(c, 0xffffffffull);
 }
 
-// The build after the tile count: emit (indices, row_indices, indptr, cell prefixes, the
-// tiles zeroed), fill, row masks -- all against `cap` tiles, the device tile count deciding
-// (more than cap: nothing is built and the overflow flag is set).
+// The build after the tile count: emit (indices, row_indices, indptr, the (cell word, tile
+// prefix) pairs, the tiles zeroed), fill, row masks and, when reserved, the row index of
+// the row-wise count (built on the device when the union averages 8 or more tiles per row
+// block) -- all against `cap` tiles, the device tile count deciding (more than cap:
+// nothing is built and the overflow flag is set).
 static int batch_enqueue_tiles(btc_batch* b, const int32_t* d_src, const int32_t* d_dst, int64_t m,
                                uint32_t cap, cudaStream_t s)
 {
@@ -286,7 +280,7 @@ static int batch_enqueue_tiles(btc_batch* b, const int32_t* d_src, const int32_t
     if (words)
         bt::k_emit_b<<<(unsigned)chunks, bt::kThreads, 0, s>>>(
             g->bitmap.as<uint32_t>(), words, dsegs, b->bm_off.as<uint64_t>(), G,
-            g->tile_base.as<uint32_t>(), g->prefix.as<uint32_t>(), g->indices.as<uint32_t>(),
+            g->tile_base.as<uint32_t>(), g->prefix.as<uint2>(), g->indices.as<uint32_t>(),
             g->row_indices.as<uint32_t>(), g->indptr.as<uint32_t>(), meta + kMetaTiles, cap,
             g->blocks.as<uint4>(), vec4);
     bt::k_set_last_b<<<1, 1, 0, s>>>(g->indptr.as<uint32_t>(), rows, meta, cap);
@@ -294,16 +288,24 @@ static int batch_enqueue_tiles(btc_batch* b, const int32_t* d_src, const int32_t
         const int egrid = grid_for((m + 3) / 4, bt::kThreads);
         if (g->tile_cols == 128)
             bt::k_fill_b<7><<<egrid, bt::kThreads, 0, s>>>(d_src, d_dst, m, dsegs, deoff, G,
-                                                           g->bitmap.as<uint32_t>(), g->prefix.as<uint32_t>(),
-                                                           g->blocks.as<uint32_t>(), meta + kMetaTiles, cap);
+                                                           g->prefix.as<uint2>(), g->blocks.as<uint32_t>(),
+                                                           meta + kMetaTiles, cap);
         else
             bt::k_fill_b<5><<<egrid, bt::kThreads, 0, s>>>(d_src, d_dst, m, dsegs, deoff, G,
-                                                           g->bitmap.as<uint32_t>(), g->prefix.as<uint32_t>(),
-                                                           g->blocks.as<uint32_t>(), meta + kMetaTiles, cap);
+                                                           g->prefix.as<uint2>(), g->blocks.as<uint32_t>(),
+                                                           meta + kMetaTiles, cap);
     }
     BTC_TRY(launch_rowmask(g->tile_cols, g->blocks.as<uint32_t>(), cap, meta + kMetaTiles,
                            g->indptr.as<uint32_t>(), g->n_row_blocks, g->rowmask.as<uint32_t>(),
                            meta + kMetaRowMax, s));
+    if (b->row_index) {
+        unsigned long long* total = g->row_bsum.as<unsigned long long>();
+        BTC_TRY(launch_rowindex(g->indptr.as<uint32_t>(), g->indices.as<uint32_t>(), g->n_row_blocks,
+                                g->rowmask.as<uint32_t>(), meta + kMetaTiles, cap,
+                                g->row_tot.as<uint32_t>(), reinterpret_cast<uint32_t*>(total + 1), total,
+                                g->row_off.as<uint32_t>(), g->row_ent.as<uint2>(),
+                                g->row_ent.bytes / sizeof(uint2), s));
+    }
     return cudaGetLastError() == cudaSuccess ? BTC_OK : BTC_E_CUDA;
 }
 
@@ -424,7 +426,7 @@ static int batch_build_into(btc_batch* b, const int32_t* src, const int32_t* dst
     }
     b->h_rowoff[(size_t)G] = (uint32_t)rows;
     b->h_bmoff[(size_t)G] = words;
-    if (words * 8 > (4ull << 30)) return BTC_E_INVAL;  // bitmap + prefix budget
+    if (words * 8 > (4ull << 30)) return BTC_E_INVAL;  // cell words: at most 512M (bitmap + pairs 6 GB)
 
     BTC_CUDA_TRY(cudaGetDevice(&g->device));
     g->tile_cols = tile_cols;
@@ -473,7 +475,7 @@ static int batch_build_into(btc_batch* b, const int32_t* src, const int32_t* dst
     // ---- mark, count, scan; the tile count to size the arrays ----------------------
     const size_t chunks = (size_t)((words + bt::kChunk - 1) / bt::kChunk);
     BTC_TRY(g->bitmap.reserve(sizeof(uint32_t) * (words ? words : 1)));
-    BTC_TRY(g->prefix.reserve(sizeof(uint32_t) * (words ? words : 1)));
+    BTC_TRY(g->prefix.reserve(sizeof(uint2) * (words ? words : 1)));
     BTC_TRY(g->tile_base.reserve(sizeof(uint32_t) * (chunks + 1)));
     BTC_TRY(batch_enqueue_mark(b, d_src, d_dst, m, s));
     if (!words && m > 0) return BTC_E_RANGE;  // only empty graphs: every edge is out of range
@@ -492,6 +494,16 @@ static int batch_build_into(btc_batch* b, const int32_t* src, const int32_t* dst
     BTC_TRY(g->row_indices.reserve(sizeof(uint32_t) * (tiles ? tiles : 1)));
     BTC_TRY(g->blocks.reserve(sizeof(uint32_t) * TW * (tiles ? tiles : 1)));
     BTC_TRY(g->rowmask.reserve(sizeof(uint32_t) * (tiles ? tiles : 1)));
+    // the row-wise count's row index, when the union averages 8 or more tiles per row
+    // block (then it has at least 8 edges per row block)
+    b->row_index = rows > 0 && (uint64_t)tiles >= 8ull * rows && m < (int64_t)0xffffffffll;
+    if (b->row_index) {
+        BTC_TRY(g->row_off.reserve(sizeof(uint32_t) * (16 * (size_t)rows + 1)));
+        BTC_TRY(g->row_ent.reserve(sizeof(uint2) * (size_t)m));
+        BTC_TRY(g->row_tot.reserve(sizeof(uint32_t) * (size_t)rows));
+        BTC_TRY(g->row_bsum.reserve(sizeof(unsigned long long) +
+                                    sizeof(uint32_t) * ((size_t)ri_scan_blocks((uint32_t)rows) + 1)));
+    }
     BTC_TRY(ensure_count_scratch(g));
     BTC_TRY(b->counts.reserve(sizeof(unsigned long long) * (size_t)G));
     BTC_TRY(batch_enqueue_tiles(b, d_src, d_dst, m, (uint32_t)tiles, s));
@@ -575,9 +587,12 @@ int btc_batch_count(btc_batch* b, int tau, btc_stream_t stream, unsigned long lo
                          g->row_indices.as<uint32_t>(), g->blocks.as<uint32_t>(),
                          b->pending ? b->pending_cap : g->num_tiles, g->n_row_blocks, tau, scr,
                          stream, b->row_off.as<uint32_t>(), (uint32_t)b->num_graphs, counts,
-                         g->rowmask.as<uint32_t>(), nullptr, 0,
+                         g->rowmask.as<uint32_t>(), g->prefix.as<uint2>(), 0,
                          g->meta.as<unsigned long long>() + kMetaRowMax, 0, 0xffffffffu, build_meta,
-                         g->num_tiles));
+                         g->num_tiles,
+                         b->row_index ? g->row_off.as<uint32_t>() : nullptr,
+                         b->row_index ? g->row_ent.as<uint2>() : nullptr, false,
+                         b->segs.as<GraphSeg>()));
     if (h_counts) {
         BTC_CUDA_TRY(cudaMemcpyAsync(h_counts, counts, bytes, cudaMemcpyDeviceToHost, stream));
         BTC_CUDA_TRY(cudaStreamSynchronize(stream));

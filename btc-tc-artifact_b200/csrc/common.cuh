@@ -150,6 +150,20 @@ BuildGeom make_geom(int32_t n, int tile_cols);
 // ---------------------------------------------------------------------------
 // Count (count.cu)
 // ---------------------------------------------------------------------------
+// One graph of a batch union: its rows, vertex ids and the part of the cell bitmap (and
+// of the (cell word, tile prefix) pairs) that covers it.  The cell of union row block J and
+// union column block K is word bm_off + (J - row_off) * wpr + ((K - cb_lo) >> 5), bit
+// (K - cb_lo) & 31; a single graph is the one segment {0, n, 0, 0, words per row, 0, 0}.
+struct GraphSeg {
+    uint32_t row_off;  // first global row block
+    int32_t n;         // vertices (local ids are in [0, n))
+    uint32_t vbase;    // first global vertex id (16 * row_off)
+    uint32_t cb_lo;    // first global column block of the graph's vertex range
+    uint32_t wpr;      // bitmap words per row block
+    uint32_t pad;
+    uint64_t bm_off;   // first bitmap word of the graph
+};
+
 struct CountScratch {
     unsigned long long* partials;  // one per CTA of the persistent grid
     unsigned int* done;            // CTAs finished (reset to 0 by the last one)
@@ -175,7 +189,7 @@ int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
                  uint32_t tile_begin = 0, uint32_t tile_end = 0xffffffffu,
                  const unsigned long long* build_meta = nullptr, uint32_t tiles_hint = 0,
                  const uint32_t* row_off = nullptr, const uint2* row_ent = nullptr,
-                 bool dense_tiles = false);
+                 bool dense_tiles = false, const GraphSeg* segs = nullptr);
 
 // rowmask[t] bit r = tile t's row r has a bit, for t < T = *d_tiles (T = cap when d_tiles
 // is null) when T >= 8 * n_row_blocks (the heavy count variant's condition), and

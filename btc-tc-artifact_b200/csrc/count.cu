@@ -827,7 +827,8 @@ int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
                  const uint32_t* rowmask, const uint2* cellpp,
                  uint64_t cell_wpr, const unsigned long long* row_max, uint32_t tile_begin,
                  uint32_t tile_end, const unsigned long long* build_meta, uint32_t tiles_hint,
-                 const uint32_t* row_off, const uint2* row_ent, bool dense_tiles)
+                 const uint32_t* row_off, const uint2* row_ent, bool dense_tiles,
+                 const GraphSeg* segs)
 {
     // build_meta: num_tiles is a capacity bound and the kernel reads the device tile
     // count; the schedule and the variant follow tiles_hint (the previous build's count)
@@ -874,7 +875,9 @@ int launch_count(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
         return launch_count_rows(tile_cols, indptr, indices, row_indices, blocks, num_tiles, tile_begin,
                                  tile_end, n_row_blocks, tau, chunk_rows, scr, graph_rows,
                                  num_graphs, graph_counts, rowmask, cellpp, cell_wpr, row_off, row_ent,
-                                 build_meta, dense_tiles, grid_all, s);
+                                 segs, build_meta, dense_tiles, grid_all, s);
+    // the tile-wise kernel indexes the cell pairs of a single graph only
+    if (segs) cellpp = nullptr;
 #define BTC_LAUNCH_COUNT(CC, HH)                                                              \
     k_count<CC, HH><<<grid, kThreads, 0, s>>>(indptr, indices, row_indices, blocks, num_tiles, \
                                               tile_begin, tile_end, n_row_blocks, tau,         \

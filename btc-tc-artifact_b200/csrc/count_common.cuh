@@ -146,7 +146,7 @@ int launch_count_rows(int tile_cols, const uint32_t* indptr, const uint32_t* ind
                       uint32_t chunk, CountScratch scr, const uint32_t* graph_rows,
                       uint32_t num_graphs, unsigned long long* graph_counts,
                       const uint32_t* rowmask, const uint2* cellpp, uint64_t cell_wpr,
-                      const uint32_t* row_off, const uint2* row_ent,
+                      const uint32_t* row_off, const uint2* row_ent, const GraphSeg* segs,
                       const unsigned long long* build_meta, bool dense, int grid, cudaStream_t s);
 
 }  // namespace btc200

@@ -32,7 +32,8 @@
 //    by cp.async into a four-tile ring per warp.  Integer arithmetic only; per-lane uint64
 //    partials and the last-CTA reduction of count_common.cuh.
 //
-// Needs the cell bitmap's (word, prefix) pairs (the bitmap builder's).  Without the row
+// Needs the cell bitmap's (word, prefix) pairs (the bitmap builder's); a batch union
+// passes the segment of each graph, whose part of the bitmap holds the cells of its rows.  Without the row
 // masks and row index at run time (an asynchronous rebuild that left fewer than 8 tiles
 // per row block) a group's units are all tiles of row block I up to S, with the mask
 // check when masks exist.
@@ -70,7 +71,8 @@ constexpr size_t rows_smem_bytes() { return sizeof(RowSmem<C>) * kRWarps; }
 // take five (48 registers; R-MAT s22 20.85 ms against 21.89 at four: the dependent-load
 // chains want every warp they can get), graphs of dense 16x128 tiles four (64 registers:
 // K_4096 on the tensor-core path 0.19 ms against 0.23 at five), 16x32 four.
-template <int C, int kMinBlocks>
+// kSeg: a batch union, whose cells are looked up in each graph's part of the bitmap.
+template <int C, int kMinBlocks, bool kSeg>
 __global__ void __launch_bounds__(kRThreads, kMinBlocks)
 k_count_rows(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ indices,
              const uint32_t* __restrict__ row_indices, const uint32_t* __restrict__ blocks,
@@ -79,7 +81,7 @@ k_count_rows(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ i
              uint32_t num_graphs, unsigned long long* __restrict__ graph_counts,
              const uint32_t* __restrict__ rowmask, const uint2* __restrict__ cellpp,
              uint64_t cell_wpr, const uint32_t* __restrict__ row_off, const uint2* __restrict__ row_ent,
-             const unsigned long long* __restrict__ build_meta)
+             const GraphSeg* __restrict__ segs, const unsigned long long* __restrict__ build_meta)
 {
     using K = Cfg<C>;
     constexpr int WPR = K::WPR, TW = K::TW, JPT = K::JPT;
@@ -105,6 +107,21 @@ k_count_rows(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ i
     const bool have_rm = rowmask != nullptr && (uint64_t)num_tiles >= 8ull * (uint64_t)(R > 0 ? R : 0);
     const bool have_ri = have_rm && row_off != nullptr && row_ent != nullptr;
     auto rmask_of = [&](uint32_t t) -> uint32_t { return have_rm ? __ldg(rowmask + t) : 0xFFFFu; };
+
+    // The (cell word, tile prefix) pair of row block J, column block K, and K's bit in it.
+    // A batch union looks the cell up in the part of the bitmap of J's graph (sg, the
+    // segment of the row block being counted); a single graph is one segment.
+    GraphSeg sg{0u, 0, 0u, 0u, (uint32_t)cell_wpr, 0u, 0ull};
+    auto cell = [&](uint32_t J, uint32_t K, uint32_t& bit) -> uint64_t {
+        if constexpr (kSeg) {
+            const uint32_t k = K - sg.cb_lo;
+            bit = 1u << (k & 31u);
+            return sg.bm_off + (uint64_t)(J - sg.row_off) * sg.wpr + (k >> 5);
+        } else {
+            bit = 1u << (K & 31u);
+            return (uint64_t)J * cell_wpr + (K >> 5);
+        }
+    };
 
     unsigned long long acc = 0, acc_total = 0;
     uint32_t g_cur = 0xffffffffu;
@@ -193,13 +210,16 @@ k_count_rows(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ i
                 }
             }
             uint2 cp[2];
+            uint32_t bits[2];
 #pragma unroll
-            for (int q = 0; q < 2; ++q)
-                cp[q] = ok[q] ? cellpp[(uint64_t)s.gJ[gg[q]] * cell_wpr + (Kb[q] >> 5)] : make_uint2(0u, 0u);
+            for (int q = 0; q < 2; ++q) {
+                const uint64_t w = cell(s.gJ[gg[q]], Kb[q], bits[q]);
+                cp[q] = ok[q] ? cellpp[w] : make_uint2(0u, 0u);
+            }
             uint32_t pb[2], m[2];
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
-                const uint32_t bit = 1u << (Kb[q] & 31u);
+                const uint32_t bit = bits[q];
                 pb[q] = cp[q].y + __popc(cp[q].x & (bit - 1u));
                 m[q] = (cp[q].x & bit) ? rmask_of(pb[q]) & rc[q] & 0xFFFFu : 0u;
             }
@@ -254,8 +274,8 @@ k_count_rows(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ i
                 uint32_t pb = 0;
                 if (i < y) {
                     const uint32_t Kb = indices[a0 + i];
-                    const uint2 cp = cellpp[(uint64_t)J * cell_wpr + (Kb >> 5)];
-                    const uint32_t bit = 1u << (Kb & 31u);
+                    uint32_t bit;
+                    const uint2 cp = cellpp[cell(J, Kb, bit)];
                     found = (cp.x & bit) != 0u;
                     pb = cp.y + __popc(cp.x & (bit - 1u));
                 }
@@ -373,6 +393,7 @@ k_count_rows(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ i
                         if (gI != g_cur) {
                             flush_graph(acc, acc_total, graph_counts, g_cur, lane);
                             g_cur = gI;
+                            if constexpr (kSeg) sg = segs[gI];
                         }
                     }
                     curI = I;
@@ -445,26 +466,36 @@ k_count_rows(const uint32_t* __restrict__ indptr, const uint32_t* __restrict__ i
 }
 
 
-using RowsKernel = decltype(&k_count_rows<128, 5>);
+using RowsKernel = decltype(&k_count_rows<128, 5, false>);
 
-// variant 0: 16x128 sparse, 1: 16x128 dense, 2: 16x32
+// variant 0: 16x128 sparse, 1: 16x128 dense, 2: 16x32; 3-5: the same for batch unions
 RowsKernel rows_kernel(int v)
 {
-    return v == 0 ? k_count_rows<128, 5> : v == 1 ? k_count_rows<128, 4> : k_count_rows<32, 4>;
+    switch (v) {
+    case 0: return k_count_rows<128, 5, false>;
+    case 1: return k_count_rows<128, 4, false>;
+    case 2: return k_count_rows<32, 4, false>;
+    case 3: return k_count_rows<128, 5, true>;
+    case 4: return k_count_rows<128, 4, true>;
+    default: return k_count_rows<32, 4, true>;
+    }
 }
 
-int rows_variant(int tile_cols, bool dense) { return tile_cols == 128 ? (dense ? 1 : 0) : 2; }
+int rows_variant(int tile_cols, bool dense, bool seg)
+{
+    return (seg ? 3 : 0) + (tile_cols == 128 ? (dense ? 1 : 0) : 2);
+}
 
 // Resident CTAs per SM of a row-wise kernel variant (dynamic shared memory above 48 KB is
 // an opt-in per function, set here once per device); 0 on error.
 int rows_variant_blocks_per_sm(int v)
 {
-    static std::atomic<int> resident[64][3];
+    static std::atomic<int> resident[64][6];
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
     int per_sm = resident[dev][v].load(std::memory_order_acquire);
     if (per_sm > 0) return per_sm;
-    const size_t smem = v == 2 ? rows_smem_bytes<32>() : rows_smem_bytes<128>();
+    const size_t smem = v % 3 == 2 ? rows_smem_bytes<32>() : rows_smem_bytes<128>();
     const RowsKernel k = rows_kernel(v);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kRThreads, smem);
@@ -482,9 +513,13 @@ int rows_variant_blocks_per_sm(int v)
 // width runs (what a count's scratch must hold partial sums for); 0 on error.
 int rows_blocks_per_sm(int tile_cols)
 {
-    const int a = rows_variant_blocks_per_sm(rows_variant(tile_cols, false));
-    const int b = rows_variant_blocks_per_sm(rows_variant(tile_cols, true));
-    return a > b ? a : b;
+    int most = 0;
+    for (bool seg : {false, true})
+        for (bool dense : {false, true}) {
+            const int p = rows_variant_blocks_per_sm(rows_variant(tile_cols, dense, seg));
+            most = p > most ? p : most;
+        }
+    return most;
 }
 
 int launch_count_rows(int tile_cols, const uint32_t* indptr, const uint32_t* indices,
@@ -493,20 +528,20 @@ int launch_count_rows(int tile_cols, const uint32_t* indptr, const uint32_t* ind
                       uint32_t chunk, CountScratch scr, const uint32_t* graph_rows,
                       uint32_t num_graphs, unsigned long long* graph_counts,
                       const uint32_t* rowmask, const uint2* cellpp, uint64_t cell_wpr,
-                      const uint32_t* row_off, const uint2* row_ent,
+                      const uint32_t* row_off, const uint2* row_ent, const GraphSeg* segs,
                       const unsigned long long* build_meta, bool dense, int grid, cudaStream_t s)
 {
     // the persistent grid is this kernel's resident CTAs, at most `grid` (the CTAs the
     // caller's scratch holds a partial sum for)
-    const int v = rows_variant(tile_cols, dense);
-    const size_t smem = v == 2 ? rows_smem_bytes<32>() : rows_smem_bytes<128>();
+    const int v = rows_variant(tile_cols, dense, segs != nullptr);
+    const size_t smem = v % 3 == 2 ? rows_smem_bytes<32>() : rows_smem_bytes<128>();
     const int per_sm = rows_variant_blocks_per_sm(v);
     if (per_sm < 1) return BTC_E_CUDA;
     if (per_sm * device_sm_count() < grid) grid = per_sm * device_sm_count();
     rows_kernel(v)<<<grid, kRThreads, smem, s>>>(indptr, indices, row_indices, blocks, num_tiles,
                                                  tile_begin, tile_end, n_row_blocks, tau, chunk, scr,
                                                  graph_rows, num_graphs, graph_counts, rowmask,
-                                                 cellpp, cell_wpr, row_off, row_ent, build_meta);
+                                                 cellpp, cell_wpr, row_off, row_ent, segs, build_meta);
     return cudaGetLastError() == cudaSuccess ? BTC_OK : BTC_E_CUDA;
 }
 
