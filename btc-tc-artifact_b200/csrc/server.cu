@@ -141,6 +141,24 @@ size_t slot_budget_in_use(btc_server* s, const Slot* except)
 
 // Device bytes a batch of m edges over `rows` row blocks may need (builder workspace,
 // bitmap, tiles at most one per edge), used to admit requests before building.
+// Cell-bitmap words of a request's part of a batch (row blocks x column-block words); a
+// batch holds at most kBatchWords of them, and a request of more than kSoloWords (a
+// large vertex range, however few its edges) runs alone through the single-graph builder,
+// which falls back to sorting when a bitmap would be too large.
+constexpr int64_t kBatchWords = 1ll << 29;
+constexpr int64_t kSoloWords = 1ll << 26;
+int64_t cell_words(int32_t n, int tile_cols)
+{
+    const int64_t rows = ((int64_t)n + 15) / 16;
+    const int64_t cbs = ((int64_t)n + tile_cols - 1) / tile_cols;
+    return rows * ((cbs + 31) / 32);
+}
+
+bool runs_alone(const btc_server* s, const Request& q, int tile_cols)
+{
+    return q.m >= s->cfg.solo_edges || cell_words(q.n, tile_cols) > kSoloWords;
+}
+
 size_t batch_bytes_bound(int64_t m, int64_t rows, int tile_cols)
 {
     const size_t tw_bytes = (size_t)2 * tile_cols;  // 16 rows x tile_cols bits
@@ -239,7 +257,7 @@ int launch_slot(btc_server* s, Slot& sl)
          cudaMemcpyAsync(dd, hd, sizeof(int32_t) * (size_t)staged, cudaMemcpyHostToDevice,
                          sl.stream) != cudaSuccess))
         return BTC_E_CUDA;
-    const bool solo = G == 1 && sl.reqs[0].m >= s->cfg.solo_edges;
+    const bool solo = G == 1 && runs_alone(s, sl.reqs[0], s->cfg.tile_cols ? s->cfg.tile_cols : 128);
     sl.solo_launch = solo;
     if (solo) {
         // a large graph gains nothing from batching; descending-degree orientation keeps
@@ -338,7 +356,7 @@ void engine_loop(btc_server* s)
                                           : 0;
                 sl.offsets.assign(1, 0);
                 sl.nv.clear();
-                int64_t m = 0, rows = 0;
+                int64_t m = 0, rows = 0, words = 0;
                 const int tile = s->cfg.tile_cols ? s->cfg.tile_cols : 128;
                 // A batch under way passes over large requests (they run alone when they
                 // reach the front), looking at most this many queued requests.
@@ -350,14 +368,16 @@ void engine_loop(btc_server* s)
                     Request& q = *it;
                     const int64_t qm = q.m;
                     // a large request runs alone (solo path), when the solo handle is free
-                    if (qm >= s->cfg.solo_edges && (!sl.reqs.empty() || s->solo_slot >= 0)) {
+                    const bool alone = runs_alone(s, q, tile);
+                    if (alone && (!sl.reqs.empty() || s->solo_slot >= 0)) {
                         ++it;
                         continue;
                     }
                     const int64_t qr = ((int64_t)q.n + 15) / 16;
                     const size_t need = batch_bytes_bound(m + qm, rows + qr, tile);
+                    const int64_t qw = cell_words(q.n, tile);
                     if (!sl.reqs.empty() &&
-                        (m + qm > s->cfg.max_batch_edges || need > budget))
+                        (m + qm > s->cfg.max_batch_edges || need > budget || words + qw > kBatchWords))
                         break;
                     if (sl.reqs.empty() && batch_bytes_bound(qm, qr, tile) > budget &&
                         others == 0) {
@@ -375,11 +395,12 @@ void engine_loop(btc_server* s)
                     if (sl.reqs.empty() && batch_bytes_bound(qm, qr, tile) > budget) break;
                     m += qm;
                     rows += qr;
+                    words += qw;
                     sl.reqs.push_back(std::move(q));
                     sl.offsets.push_back(m);
                     sl.nv.push_back(sl.reqs.back().n);
                     it = s->pending.erase(it);
-                    if (qm >= s->cfg.solo_edges) {
+                    if (alone) {
                         s->solo_slot = (int)(&sl - s->slots.data());
                         break;
                     }

@@ -353,8 +353,9 @@ typedef struct btc_server_config {
     int64_t max_batch_edges;   /* input edges per batch */
     int tile_cols;             /* 32, 128, or 0 for the engine's tile policy per batch */
     int tau;                   /* dense/sparse switch, BTC_TAU_DEFAULT */
-    int64_t solo_edges;        /* requests with at least this many edges run alone,
-                                  degree-ordered, with the engine's tile policy */
+    int64_t solo_edges;        /* requests with at least this many edges (or a vertex
+                                  range needing more than 2^26 cell-bitmap words) run
+                                  alone, degree-ordered, with the engine's tile policy */
 } btc_server_config;
 
 typedef struct btc_server_result {

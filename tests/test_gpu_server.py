@@ -157,3 +157,27 @@ def test_server_recovers_from_injected_allocation_failures(monkeypatch):
                 assert res[0]["status"] == 0 and res[0]["count"] == want[k], (k, res)
     finally:
         srv.close()
+
+
+def test_sparse_graphs_on_large_vertex_ranges_in_the_mix():
+    """A request's cell bitmap grows with its vertex range, not its edges: graphs of two
+    million vertices and a few thousand edges, with the edge threshold for running alone
+    raised so that only their vertex range sends them there, mixed with small graphs,
+    still count exactly (a batch holding several of them would need more cell words than
+    a batch may hold)."""
+    rng = np.random.default_rng(17)
+    gs = _pool()
+    for k in range(4):
+        n = 1 << 21
+        hub = rng.integers(0, n, 64)
+        s = np.concatenate([hub[rng.integers(0, 64, 3000)], rng.integers(0, n, 1000)]).astype(np.int32)
+        d = np.concatenate([hub[rng.integers(0, 64, 3000)], rng.integers(0, n, 1000)]).astype(np.int32)
+        gs.append((s, d, n))
+    want = _reference(gs)
+    order = list(rng.permutation(len(gs))) * 2
+    srv = Server(slots=2, max_batch_graphs=4096, solo_edges=1 << 24)
+    try:
+        for k, c in _run(srv, gs, order):
+            assert c == want[k], k
+    finally:
+        srv.close()
