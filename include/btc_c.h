@@ -302,7 +302,9 @@ typedef struct btc_batch btc_batch; /* opaque, device-resident */
  * BTC_INPUT_ON_HOST.  The batch is the block-diagonal union of the graphs (graph g's
  * vertex v is union vertex 16*R_<g + v, R_<g = row blocks of graphs 0..g-1), with one
  * tile width for all (32, 128, or 0 for btc_select_tile_policy over the whole batch, each
- * sampled edge's locality measured against its own graph's size).
+ * sampled edge's locality measured against its own graph's size).  Each graph has its own
+ * cell bitmap of ceil(n/16) x ceil(ceil(n/tile_cols)/32) words; a batch whose graphs need
+ * more than 2^29 words together returns BTC_E_INVAL (count such graphs one at a time).
  * Synchronises `stream` once. */
 BTC_API int btc_batch_build(const int32_t* src, const int32_t* dst, const int64_t* edge_offsets,
                             const int32_t* num_vertices, int32_t num_graphs, int tile_cols,
