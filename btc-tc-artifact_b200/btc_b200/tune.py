@@ -89,6 +89,12 @@ def autotune(src, dst, n: int, orient_degree: bool = False, tiles=(32, 128), rep
     return {"tile_cols": best, "count": count, "lite_policy": lite, "table": table}
 
 
+def _mix_graph(index: int):
+    from . import graphs as G
+    s, d, _, nv, _ = G.batch_mix_device(4096, 256, 65536, seed=11, select=[index])
+    return s, d, int(nv[0])
+
+
 def standard_graphs(names=None):
     from . import graphs as G
     makers = {"stencil27_64": lambda: G.stencil27(64),
@@ -99,7 +105,10 @@ def standard_graphs(names=None):
               # dedups), generated on the GPU
               "rmat_raw18_deg": lambda: G.rmat_raw_torch(18, 16, 7),
               "rmat_raw20_deg": lambda: G.rmat_raw_torch(20, 16, 21),
-              "rmat_raw22_deg": lambda: G.rmat_raw_torch(22, 16, 7)}
+              "rmat_raw22_deg": lambda: G.rmat_raw_torch(22, 16, 7),
+              # the largest graph of the bench's 4096-graph batched mix (seed 11, graph 1742:
+              # an 8-community SBM, n = 60,747, 68.3M raw pairs), generated on the GPU
+              "sbm_mix1742": lambda: _mix_graph(1742)}
     names = names or ["stencil27_64", "er_16384_16", "rmat18_deg"]
     return [(k, makers[k](), k.endswith("_deg")) for k in names]
 
