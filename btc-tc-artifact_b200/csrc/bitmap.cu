@@ -112,32 +112,63 @@ __device__ __forceinline__ void load_words(const uint32_t* __restrict__ bitmap, 
     for (int k = 0; k < WPT; ++k) x[k] = (w0 + k < W) ? bitmap[w0 + k] : 0u;
 }
 
-// The same for k_bm_emit, reading only the words that can hold a cell.  Edges are
-// oriented (max, min), so row block rb's cells lie in column blocks <= (16 rb + 15) >>
-// LOG2C and its words past (16 rb + 15) >> (LOG2C + 5) (lshift = LOG2C + 5) stay zero:
-// about half of the bitmap, whose pairs k_bm_emit need not write since no lookup lands
-// there (a lookup of row block J, column block K always has K within J's lower triangle).
-// Bit k of the result: word w0 + k can hold a cell.  The builder takes this path only for
-// bitmaps of at most 2^30 words (4 GiB), so word and row indices fit 32 bits.  (The chunk
-// popcount keeps plain loads: the per-thread row arithmetic cost it more than the skipped
-// reads saved, 341 against 292 us at R-MAT s22.)
+// Division of word indices by the words per row without a divide instruction: for
+// n < 2^31 and d > 1, n / d = umulhi(n, m) >> s with l = ceil(log2 d), m = ceil(2^(31+l) / d)
+// (< 2^32) and s = l - 1 (Granlund and Montgomery, "Division by invariant integers using
+// multiplication", 1994, theorem 4.2 with N = 31); d = 1 is passed through.
+struct RowDiv {
+    uint32_t d, m, s;
+};
+
+inline RowDiv make_row_div(uint64_t d)
+{
+    RowDiv v{(uint32_t)d, 0u, 0u};
+    if (d > 1) {
+        uint32_t l = 0;
+        while ((1ull << l) < d) ++l;
+        v.m = (uint32_t)(((1ull << (31 + l)) + d - 1) / d);
+        v.s = l - 1;
+    }
+    return v;
+}
+
+__device__ __forceinline__ uint32_t row_of(uint32_t n, RowDiv v)
+{
+    return v.d == 1 ? n : (__umulhi(n, v.m) >> v.s);
+}
+
+// Reading only the words that can hold a cell.  Edges are oriented (max, min), so row
+// block rb's cells lie in column blocks <= (16 rb + 15) >> LOG2C and its words past
+// (16 rb + 15) >> (LOG2C + 5) (lshift = LOG2C + 5) stay zero: about half of the bitmap,
+// which the chunk popcount need not read and k_bm_emit need not give pairs, since no
+// lookup lands there (a lookup of row block J, column block K always has K within J's
+// lower triangle).  Bit k of the result: word w0 + k can hold a cell.  The builder takes
+// this path only for bitmaps of at most 2^30 words (4 GiB), so word and row indices fit
+// 31 bits.  The usual thread's WPT words lie in one row and take the short path; per-word
+// arithmetic with a divide instruction made the chunk popcount slower than reading
+// everything (341 against 292 us at R-MAT s22).
 template <int WPT>
 __device__ __forceinline__ uint32_t load_lower_words(const uint32_t* __restrict__ bitmap, uint64_t w0,
-                                                     uint64_t W, uint64_t wpr, uint32_t lshift,
+                                                     uint64_t W, RowDiv wpr, uint32_t lshift,
                                                      uint32_t (&x)[WPT])
 {
-    const uint32_t wpr32 = (uint32_t)wpr;
-    uint32_t rb = (uint32_t)w0 / wpr32;
-    uint32_t cw = (uint32_t)w0 - rb * wpr32;
+    constexpr uint32_t kAll = WPT == 32 ? 0xFFFFFFFFu : (1u << WPT) - 1u;
+    uint32_t rb = row_of((uint32_t)w0, wpr);
+    uint32_t cw = (uint32_t)w0 - rb * wpr.d;
     uint32_t lim = (16u * rb + 15u) >> lshift;
     uint32_t need = 0;
+    if (w0 + WPT <= W && cw + WPT <= wpr.d) {
+        // one row: the words up to lim
+        if (cw <= lim) need = lim - cw + 1u >= (uint32_t)WPT ? kAll : (1u << (lim - cw + 1u)) - 1u;
+    } else {
 #pragma unroll
-    for (int k = 0; k < WPT; ++k) {
-        if (w0 + k < W && cw <= lim) need |= 1u << k;
-        if (++cw == wpr32) {
-            cw = 0;
-            ++rb;
-            lim = (16u * rb + 15u) >> lshift;
+        for (int k = 0; k < WPT; ++k) {
+            if (w0 + k < W && cw <= lim) need |= 1u << k;
+            if (++cw == wpr.d) {
+                cw = 0;
+                ++rb;
+                lim = (16u * rb + 15u) >> lshift;
+            }
         }
     }
     if constexpr (WPT % 4 == 0) {
@@ -184,8 +215,8 @@ k_bm_count(const uint32_t* __restrict__ bitmap, uint64_t W, uint32_t* __restrict
 // bases and writes the tile total to meta[kMetaTiles].  No CTA waits for another.
 template <int WPT>
 __global__ void __launch_bounds__(kThreads)
-k_bm_count_scan(const uint32_t* __restrict__ bitmap, uint64_t W, uint32_t* chunk_base,
-                unsigned long long* meta)
+k_bm_count_scan(const uint32_t* __restrict__ bitmap, uint64_t W, RowDiv wpr, uint32_t lshift,
+                uint32_t* chunk_base, unsigned long long* meta)
 {
     __shared__ uint32_t s_warp[kThreads / kWarp];
     __shared__ unsigned long long s_tot[kThreads / kWarp];
@@ -193,7 +224,7 @@ k_bm_count_scan(const uint32_t* __restrict__ bitmap, uint64_t W, uint32_t* chunk
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t w0 = (uint64_t)blockIdx.x * (kThreads * WPT) + (uint64_t)threadIdx.x * WPT;
     uint32_t x[WPT];
-    load_words<WPT>(bitmap, w0, W, x);
+    load_lower_words<WPT>(bitmap, w0, W, wpr, lshift, x);
     uint32_t sum = 0;
 #pragma unroll
     for (int k = 0; k < WPT; ++k) sum += __popc(x[k]);
@@ -253,7 +284,7 @@ __device__ __forceinline__ void finish_tiles(uint32_t* indptr, int32_t R, unsign
 
 template <int WPT>
 __global__ void __launch_bounds__(kThreads)
-k_bm_emit(const uint32_t* __restrict__ bitmap, uint64_t W, uint64_t wpr, uint32_t lshift,
+k_bm_emit(const uint32_t* __restrict__ bitmap, uint64_t W, RowDiv wpr, uint32_t lshift,
           const uint32_t* __restrict__ chunk_base, uint2* __restrict__ cellpp,
           uint32_t* __restrict__ indices, uint32_t* __restrict__ row_indices,
           uint32_t* __restrict__ indptr, unsigned long long* meta, uint32_t cap,
@@ -295,8 +326,8 @@ k_bm_emit(const uint32_t* __restrict__ bitmap, uint64_t W, uint64_t wpr, uint32_
     for (int w = 0; w < kThreads / kWarp; ++w) base += (w < warp) ? s_warp[w] : 0u;
     if (w0 >= W) return;
 
-    uint32_t rb = (uint32_t)w0 / (uint32_t)wpr;  // at most 2^30 words (load_lower_words)
-    uint32_t col_word = (uint32_t)w0 - rb * (uint32_t)wpr;
+    uint32_t rb = row_of((uint32_t)w0, wpr);  // at most 2^30 words (load_lower_words)
+    uint32_t col_word = (uint32_t)w0 - rb * wpr.d;
     uint32_t pre[WPT];
 #pragma unroll
     for (int k = 0; k < WPT; ++k) {
@@ -314,7 +345,7 @@ k_bm_emit(const uint32_t* __restrict__ bitmap, uint64_t W, uint64_t wpr, uint32_
             }
             base = t;
         }
-        if (++col_word == wpr) {
+        if (++col_word == wpr.d) {
             col_word = 0;
             ++rb;
         }
@@ -486,15 +517,20 @@ int bitmap_mark_and_count(const BuildGeom& g, const int32_t* src, const int32_t*
     const size_t chunks = bitmap_chunks(W);
     // meta_tiles - kMetaTiles is the metadata base (its ticket slot is zero)
     unsigned long long* meta = meta_tiles - kMetaTiles;
+    const bm::RowDiv rdiv = bm::make_row_div(wpr);
+    const uint32_t lshift = (g.tile_cols == 128 ? 7u : 5u) + 5u;
     switch (bitmap_wpt(W)) {
     case 16:
-        bm::k_bm_count_scan<16><<<(unsigned)chunks, bm::kThreads, 0, s>>>(bitmap, W, chunk_count, meta);
+        bm::k_bm_count_scan<16><<<(unsigned)chunks, bm::kThreads, 0, s>>>(bitmap, W, rdiv, lshift,
+                                                                          chunk_count, meta);
         break;
     case 4:
-        bm::k_bm_count_scan<4><<<(unsigned)chunks, bm::kThreads, 0, s>>>(bitmap, W, chunk_count, meta);
+        bm::k_bm_count_scan<4><<<(unsigned)chunks, bm::kThreads, 0, s>>>(bitmap, W, rdiv, lshift,
+                                                                         chunk_count, meta);
         break;
     default:
-        bm::k_bm_count_scan<1><<<(unsigned)chunks, bm::kThreads, 0, s>>>(bitmap, W, chunk_count, meta);
+        bm::k_bm_count_scan<1><<<(unsigned)chunks, bm::kThreads, 0, s>>>(bitmap, W, rdiv, lshift,
+                                                                         chunk_count, meta);
         break;
     }
     return cudaGetLastError() == cudaSuccess ? BTC_OK : BTC_E_CUDA;
@@ -517,7 +553,8 @@ int bitmap_emit_and_fill(const BuildGeom& g, const int32_t* src, const int32_t* 
         const int R = g.n_row_blocks;
         const uint32_t lshift = (g.tile_cols == 128 ? 7u : 5u) + 5u;
 #define BTC_EMIT(WPT)                                                                         \
-    bm::k_bm_emit<WPT><<<grid, bm::kThreads, 0, s>>>(bitmap, W, wpr, lshift, chunk_base, cellpp, indices, \
+    bm::k_bm_emit<WPT><<<grid, bm::kThreads, 0, s>>>(bitmap, W, bm::make_row_div(wpr), lshift, chunk_base, \
+                                                    cellpp, indices, \
                                                     row_indices, indptr, meta, cap, host_meta, R, \
                                                     b4, vec4, rowmask)
         switch (bitmap_wpt(W)) {
