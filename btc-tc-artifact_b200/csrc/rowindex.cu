@@ -130,15 +130,21 @@ __global__ void k_ri_fill(const uint32_t* __restrict__ indptr, const uint32_t* _
     const uint64_t nw = (uint64_t)gridDim.x * (kThreads / kWarp);
     for (uint64_t I = ((uint64_t)blockIdx.x * kThreads + threadIdx.x) / kWarp; I < R; I += nw) {
         const uint32_t a = indptr[I], b = indptr[I + 1];
-        // per-row counts: lane r < 16 holds row r's
+        // per-row counts: lane r < 16 holds row r's.  Each lane's 16-bit mask is spread
+        // four rows to a word, one row per byte (a nibble times 0x00204081 puts its bit j
+        // at bit 8j), and one warp add per word sums four rows over the round's 32 tiles
+        // (at most 32 per byte, so no byte carries into the next): 4 adds where one
+        // ballot per row took 16.
         uint32_t cnt = 0;
         for (uint32_t t0 = a; t0 < b; t0 += kWarp) {
             const uint32_t m = t0 + lane < b ? rowmask[t0 + lane] : 0u;
+            uint32_t q[4];
 #pragma unroll
-            for (int r = 0; r < 16; ++r) {
-                const unsigned bl = __ballot_sync(kFull, (m >> r) & 1u);
-                if (lane == r) cnt += __popc(bl);
-            }
+            for (int k = 0; k < 4; ++k)
+                q[k] = __reduce_add_sync(kFull, (((m >> (4 * k)) & 0xFu) * 0x00204081u) & 0x01010101u);
+            const uint32_t g = (uint32_t)lane >> 2;  // lane r's word
+            const uint32_t w = g == 0 ? q[0] : g == 1 ? q[1] : g == 2 ? q[2] : q[3];
+            if (lane < 16) cnt += (w >> (8 * (lane & 3))) & 0xFFu;
         }
         uint32_t incl = cnt;
 #pragma unroll
